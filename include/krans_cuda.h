@@ -1,0 +1,278 @@
+/*
+ * krans_cuda.h - C ABI of the B200-native KraNS null-space engine
+ * (libkrans_cuda.so). Plain pointers and sizes only; no C++ or torch types.
+ *
+ * Every function returns KRANS_OK (0) or a negative KRANS_ERR_* code; no C++
+ * exception crosses this boundary. The message of the last failure on the
+ * calling thread is available from krans_last_error().
+ *
+ * Each entry point below replaces one piece of the reference's C++ plug-in
+ * API (Deep-SANE/krans, paths relative to its root):
+ *   MatrixInterface        include/krans/MatrixInterface.hpp:10-24
+ *   VectorInterface        include/krans/VectorInterface.hpp:8-34
+ *   VectorFactory          include/krans/VectorFactory.hpp:9-23
+ *   CyclicLanczosOptions / find_nullspace_cyclic_lanczos[_ex]
+ *                          include/krans/Solvers/CyclicLanczosSolver.hpp:84-178
+ *   LOBPCGOptions / find_nullspace_lobpcg[_ex]
+ *                          include/krans/Solvers/LOBPCGSolver.hpp:71-149
+ * The header-only C++ adapters in include/krans/adapters/cuda/ bind these
+ * functions back to the reference's class interfaces.
+ *
+ * Threading: a context owns one CUDA stream; calls on one context must not
+ * overlap from several host threads. Use one context per host thread.
+ */
+#ifndef KRANS_CUDA_H
+#define KRANS_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------------- */
+#define KRANS_OK 0
+#define KRANS_ERR_INVALID_ARGUMENT (-1) /* std::invalid_argument in the reference */
+#define KRANS_ERR_RUNTIME (-2)          /* std::runtime_error in the reference */
+#define KRANS_ERR_CUDA (-3)             /* a CUDA runtime call failed */
+#define KRANS_ERR_OUT_OF_MEMORY (-4)    /* device allocation or HBM budget exceeded */
+#define KRANS_ERR_TIMEOUT (-5)          /* a bounded device-side wait gave up */
+#define KRANS_ERR_NOT_FOUND (-6)        /* unknown ticket */
+#define KRANS_ERR_CANCELLED (-7)        /* request cancelled before it ran */
+
+typedef struct krans_ctx krans_ctx;
+typedef struct krans_mat krans_mat;
+typedef struct krans_vec krans_vec;
+typedef struct krans_rng krans_rng;
+
+/* Message of the last failed call on this thread ("" if none). */
+const char *krans_last_error(void);
+/* Library version string. */
+const char *krans_version(void);
+
+/* ---- context --------------------------------------------------------------- */
+/* Opens `device`, creates the context's stream. hbm_budget_bytes = 0 means
+ * no budget beyond the device's free memory. */
+int krans_ctx_create(int device, size_t hbm_budget_bytes, krans_ctx **out);
+int krans_ctx_destroy(krans_ctx *ctx);
+int krans_ctx_synchronize(krans_ctx *ctx);
+/* Bytes currently held by the context's allocations. */
+int krans_ctx_memory_in_use(const krans_ctx *ctx, size_t *bytes);
+/* Number of SMs of the context's device. */
+int krans_ctx_sm_count(const krans_ctx *ctx, int *sms);
+
+/* ---- CSR matrix: MatrixInterface (rows, cols, multiply, multiply_transpose) --
+ * Replaces EigenSparseMatrixAdapter(A), which owns A and a cached transpose
+ * (include/krans/adapters/eigen/EigenSparseMatrixAdapter.hpp:20-24,56).
+ * Host arrays are copied; the transpose is built on the device. Column
+ * indices within a row need not be sorted; duplicates are kept as given. */
+#define KRANS_CSR_FP64 1 /* keep FP64 values (needed by every FP64 path) */
+#define KRANS_CSR_FP32 2 /* also keep an FP32 copy of the values (mixed precision) */
+int krans_csr_create(krans_ctx *ctx, int64_t m, int64_t n, int64_t nnz,
+                     const int32_t *row_ptr, const int32_t *col_idx,
+                     const double *values, int flags, krans_mat **out);
+int krans_csr_destroy(krans_mat *A);
+int krans_csr_dims(const krans_mat *A, int64_t *m, int64_t *n, int64_t *nnz);
+/* Device pointers of the stored arrays (trans=1: the explicit transpose). */
+int krans_csr_device_arrays(const krans_mat *A, int trans, const int32_t **row_ptr,
+                            const int32_t **col_idx, const double **values,
+                            const float **values32);
+
+/* ---- vectors: VectorInterface (FP64, device resident) ----------------------- */
+int krans_vec_create(krans_ctx *ctx, int64_t n, krans_vec **out); /* zero-filled */
+int krans_vec_destroy(krans_vec *v);
+int krans_vec_size(const krans_vec *v, int64_t *n);
+int krans_vec_device_ptr(krans_vec *v, double **dptr);
+int krans_vec_upload(krans_vec *v, const double *host, int64_t n);
+int krans_vec_download(const krans_vec *v, double *host, int64_t n);
+int krans_vec_dot(const krans_vec *x, const krans_vec *y, double *out);   /* dot */
+int krans_vec_axpy(krans_vec *y, double alpha, const krans_vec *x);      /* add_scaled */
+int krans_vec_scale(krans_vec *v, double alpha);                         /* scale */
+int krans_vec_nrm2(const krans_vec *v, double *out);                     /* norm */
+int krans_vec_normalize(krans_vec *v);                                   /* normalize */
+int krans_vec_fill(krans_vec *v, double value);                          /* set_zero */
+int krans_vec_copy(krans_vec *dst, const krans_vec *src);                /* copy_from */
+int krans_vec_clone(const krans_vec *src, krans_vec **out);              /* clone */
+
+/* y <- A x (trans = 0) or y <- A^T x (trans = 1): multiply / multiply_transpose.
+ * precision: 0 = FP64 values, 1 = FP32 values with FP32 accumulation. */
+int krans_spmv(const krans_mat *A, int trans, const krans_vec *x, krans_vec *y);
+int krans_spmv_ex(const krans_mat *A, int trans, int precision, const krans_vec *x,
+                  krans_vec *y);
+
+/* ---- random vectors: VectorFactory::create_random_of_size ------------------
+ * KRANS_RNG_MT19937 reproduces std::mt19937(seed) + std::normal_distribution
+ * <double>(0,1) as used by StdVectorFactory/EigenVectorFactory
+ * (include/krans/adapters/universal/StdVectorFactory.hpp:16-20,38-44),
+ * including the state carried from one vector to the next. Seed 0 draws a
+ * seed from the host's random device, as the reference does.
+ * KRANS_RNG_PHILOX is a counter-based stream (Philox4x32-10 + Box-Muller):
+ * not the reference's sequence, but fully parallel. */
+#define KRANS_RNG_MT19937 0
+#define KRANS_RNG_PHILOX 1
+int krans_rng_create(krans_ctx *ctx, uint32_t seed, int mode, krans_rng **out);
+int krans_rng_destroy(krans_rng *r);
+int krans_rng_normal(krans_rng *r, krans_vec *out); /* next size(out) normals */
+int krans_rng_seed(const krans_rng *r, uint32_t *seed);
+
+/* ---- solver options (field names, meanings and defaults of the reference) -- */
+#define KRANS_PREC_FP64 0  /* plain FP64 throughout */
+#define KRANS_PREC_MIXED 1 /* FP32 SpMV + Krylov recurrence, FP64 reorth/tiny/polish */
+
+#define KRANS_TEAM_AUTO 0 /* pick by problem size */
+#define KRANS_TEAM_CTA 1  /* one thread block runs the solve */
+#define KRANS_TEAM_GRID 2 /* the whole GPU runs the solve (cooperative launch) */
+
+typedef struct krans_cyclic_opts {
+  int64_t k;                 /* 1    number of right null vectors wanted */
+  int64_t ncv;               /* 48   Krylov dimension (Lanczos vectors of H(A)) */
+  int64_t max_restarts;      /* 80 */
+  double tol_abs;            /* 1e-12 accept if ||Av|| <= max(tol_abs, tol_rel*max(1,||A||_F~)) */
+  double tol_rel;            /* 1e-10 */
+  int32_t reorth;            /* 2    ReorthMode: 0 None, 1 Single, 2 Double */
+  int32_t use_harmonic;      /* 1    refined interior extraction (else plain Ritz) */
+  double target_tau;         /* 0 */
+  int32_t nullity_known;     /* -1 */
+  int32_t rank_known;        /* -1 */
+  int64_t cg_maxit;          /* 80 */
+  double cg_rel_tol;         /* 1e-10 */
+  double cg_breakdown_tol;   /* 1e-30 */
+  int32_t projector_passes;  /* 1 */
+  int32_t grad_max_iters;    /* 3000 */
+  int32_t frob_samples;      /* 4 */
+  double prescreen_factor;   /* 0.8 */
+  int64_t stagnation_restarts; /* 30 */
+  int32_t return_left_space; /* 0 */
+  int32_t verbose;           /* 0 (device engine: ignored) */
+  /* B200 engine knobs (no reference counterpart) */
+  int32_t precision;         /* KRANS_PREC_FP64 */
+  int32_t team;              /* KRANS_TEAM_AUTO */
+} krans_cyclic_opts;
+
+typedef struct krans_cyclic_result {
+  int64_t n_right, n_left;   /* sizes of right_null / left_null */
+  int64_t restarts;          /* CyclicLanczosResult::restarts */
+  int64_t krylov_steps_total;
+  double frob_norm_est;
+  int32_t converged_to_target;
+  int32_t status;            /* KRANS_OK or a device-side error code */
+  int64_t cg_solves, cg_maxit_hits;
+  /* B200 engine diagnostics */
+  int64_t spmv, spmvT;       /* operator applications (CountingMatrixAdapter) */
+  double algo_bytes;         /* algorithmic HBM bytes of the solve */
+  double device_ms;          /* device time of the solve kernel(s) */
+} krans_cyclic_result;
+
+typedef struct krans_lobpcg_opts {
+  int64_t nev;               /* 1 */
+  int64_t block_size;        /* 0 = auto min(16, nev) */
+  int64_t max_iters;         /* 1000 */
+  double tol_abs;            /* 1e-12 */
+  double tol_rel;            /* 1e-10 */
+  int32_t soft_locking;      /* 1 */
+  double restart;            /* 0.9 */
+  double gs_tol;             /* 1e-14 */
+  int32_t gs_reorth;         /* 1 */
+  int32_t frob_samples;      /* 4 */
+  int64_t max_tiny_dim;      /* 0 */
+  int32_t nullity_known;     /* -1 */
+  int32_t rank_known;        /* -1 */
+  int32_t verbose;           /* 0 (device engine: ignored) */
+  int64_t progress_every;    /* 100 (device engine: ignored) */
+  int32_t precision;         /* KRANS_PREC_FP64 */
+  int32_t team;              /* KRANS_TEAM_AUTO */
+} krans_lobpcg_opts;
+
+typedef struct krans_lobpcg_result {
+  int64_t n_right;
+  int64_t iters, locked;
+  double frob_norm_est, accept_threshold, best_unaccepted_residual;
+  int64_t block_size;
+  int32_t converged_to_target;
+  int32_t status;
+  int64_t spmv, spmvT;
+  double algo_bytes, gram_flops;
+  double device_ms;
+} krans_lobpcg_result;
+
+int krans_cyclic_opts_init(krans_cyclic_opts *o);
+int krans_lobpcg_opts_init(krans_lobpcg_opts *o);
+
+/* find_nullspace_cyclic_lanczos_ex on the device engine
+ * (src/Solvers/CyclicLanczosSolver.cpp:618-660 in the reference).
+ * rng: the factory's stream (consumed and advanced exactly as the reference
+ *      consumes VectorFactory::create_random_of_size).
+ * initial_right: optional start vector y0 (CyclicLanczosOptions::
+ *      initial_right_space.front()), or NULL.
+ * right_out: caller array of capacity max(k, nullity_known) handles; filled
+ *      with newly created vectors owned by the caller (result->n_right).
+ * left_out: capacity k handles, used when return_left_space (may be NULL). */
+int krans_solve_cyclic(krans_ctx *ctx, const krans_mat *A, krans_rng *rng,
+                       const krans_cyclic_opts *opts, const krans_vec *initial_right,
+                       krans_vec **right_out, krans_vec **left_out,
+                       krans_cyclic_result *result);
+
+/* find_nullspace_lobpcg_ex on the device engine
+ * (src/Solvers/LOBPCGSolver.cpp:443-834 in the reference).
+ * initial_block: optional array of n_initial seed vectors, or NULL.
+ * right_out: capacity = the reference's k_target; theta_out/resid_out
+ *      (host, may be NULL) receive LOBPCGResult::theta / residuals_Av. */
+int krans_solve_lobpcg(krans_ctx *ctx, const krans_mat *A, krans_rng *rng,
+                       const krans_lobpcg_opts *opts, const krans_vec *const *initial_block,
+                       int64_t n_initial, krans_vec **right_out, double *theta_out,
+                       double *resid_out, krans_lobpcg_result *result);
+
+/* ---- batched solves: many independent requests in one persistent launch --- */
+typedef struct krans_request {
+  const krans_mat *A;        /* matrix of this request */
+  krans_cyclic_opts opts;    /* per-request options (k, tolerances, precision) */
+  uint32_t seed;             /* RNG seed of the request's own stream */
+  int32_t rng_mode;          /* KRANS_RNG_PHILOX or KRANS_RNG_MT19937 */
+  double *basis_out;         /* device or host? see krans_solve_batch */
+  int64_t basis_capacity;    /* vectors that fit in basis_out */
+} krans_request;
+
+typedef struct krans_request_result {
+  int32_t status;            /* KRANS_OK or error */
+  int32_t converged_to_target;
+  int64_t n_right;
+  int64_t restarts, krylov_steps_total, cg_solves, cg_maxit_hits;
+  int64_t spmv, spmvT;
+  double frob_norm_est;
+  double max_residual;       /* max ||A u||_2 over the returned basis (FP64) */
+  double algo_bytes;
+  double queue_ms, device_ms, latency_ms; /* serving only */
+} krans_request_result;
+
+/* Solve `count` cyclic requests in one persistent launch (one thread block
+ * per request at a time, largest first). basis_out of each request is a
+ * DEVICE pointer to basis_capacity x cols(A) doubles (row i = vector i). */
+int krans_solve_batch(krans_ctx *ctx, int64_t count, const krans_request *reqs,
+                      krans_request_result *results, double *device_ms);
+
+/* ---- serving: continuous batching against an HBM budget ---------------------- */
+typedef struct krans_server krans_server;
+typedef struct krans_server_opts {
+  size_t hbm_budget_bytes;   /* admission budget for request state (0 = 150 GB) */
+  int32_t max_inflight_launches; /* concurrent persistent launches (streams) */
+  int32_t max_batch;         /* requests per launch */
+  double batch_window_ms;    /* how long the scheduler waits to fill a launch */
+} krans_server_opts;
+
+int krans_server_opts_init(krans_server_opts *o);
+int krans_server_create(krans_ctx *ctx, const krans_server_opts *opts, krans_server **out);
+int krans_server_destroy(krans_server *s);
+/* Queue a request; the server copies the descriptor (A must stay alive until
+ * the ticket completes). basis_out is a device pointer as in krans_request. */
+int krans_submit(krans_server *s, const krans_request *req, uint64_t *ticket);
+/* status: 0 queued, 1 running, 2 done, 3 failed, 4 cancelled */
+int krans_poll(krans_server *s, uint64_t ticket, int *status, krans_request_result *result);
+int krans_cancel(krans_server *s, uint64_t ticket);
+/* Block until every submitted request has finished or timeout_ms passes. */
+int krans_server_drain(krans_server *s, double timeout_ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* KRANS_CUDA_H */

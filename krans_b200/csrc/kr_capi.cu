@@ -1,0 +1,757 @@
+// C ABI of the KraNS B200 engine: context, CSR matrices, vectors, SpMV,
+// random vectors and the single-request solver launches.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <random>
+
+#include "kr_cyclic.cuh"
+#include "kr_internal.h"
+
+namespace kr {
+
+static thread_local std::string g_last_error;
+
+void set_error(const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+}
+
+int cuda_fail(cudaError_t e, const char *what, const char *file, int line) {
+  set_error("CUDA error %s (%s) in %s at %s:%d", cudaGetErrorName(e), cudaGetErrorString(e), what,
+            file, line);
+  if (e == cudaErrorMemoryAllocation)
+    return KRANS_ERR_OUT_OF_MEMORY;
+  return KRANS_ERR_CUDA;
+}
+
+int dev_alloc(krans_ctx *ctx, void **p, size_t bytes) {
+  *p = nullptr;
+  if (bytes == 0)
+    bytes = 256;
+  if (ctx->budget && ctx->in_use + bytes > ctx->budget) {
+    set_error("HBM budget exceeded: %zu + %zu > %zu bytes", ctx->in_use, bytes, ctx->budget);
+    return KRANS_ERR_OUT_OF_MEMORY;
+  }
+  cudaError_t e = cudaMalloc(p, bytes);
+  if (e != cudaSuccess)
+    return cuda_fail(e, "cudaMalloc", __FILE__, __LINE__);
+  ctx->in_use += bytes;
+  return KRANS_OK;
+}
+
+void dev_free(krans_ctx *ctx, void *p, size_t bytes) {
+  if (!p)
+    return;
+  if (bytes == 0)
+    bytes = 256;
+  cudaFree(p);
+  ctx->in_use -= std::min(ctx->in_use, bytes);
+}
+
+int pick_lanes(int64_t rows, int64_t nnz) {
+  const double mean = rows > 0 ? (double)nnz / (double)rows : 0.0;
+  if (mean <= 1.5)
+    return 1;
+  if (mean <= 3.0)
+    return 2;
+  if (mean <= 6.0)
+    return 4;
+  if (mean <= 12.0)
+    return 8;
+  if (mean <= 24.0)
+    return 16;
+  return 32;
+}
+
+// ---------------------------------------------------------------------------
+// Flat "team" for standalone kernels: grid-stride loops, no team barriers.
+// ---------------------------------------------------------------------------
+struct TeamFlat {
+  KR_DEV int64_t tid() const { return (int64_t)blockIdx.x * blockDim.x + threadIdx.x; }
+  KR_DEV int64_t nthreads() const { return (int64_t)gridDim.x * blockDim.x; }
+  KR_DEV int64_t warp_id() const { return tid() >> 5; }
+  KR_DEV int64_t nwarps() const { return nthreads() >> 5; }
+};
+
+template <class VT, class XT, class YT>
+__global__ void __launch_bounds__(256) spmv_kernel(int64_t rows, const int32_t *rp, const int32_t *ci,
+                                                   const VT *val, const XT *x, YT *y, int lanes) {
+  TeamFlat tm;
+  team_spmv(tm, rows, rp, ci, val, x, lanes, [&](int64_t i, typename AccOf<VT>::T s) { y[i] = (YT)s; });
+}
+
+// two-stage deterministic reduction: partial per block, then one block sums
+__global__ void __launch_bounds__(256) dot_partial_kernel(int64_t n, const double *x, const double *y,
+                                                          double *part) {
+  __shared__ TeamShared sh;
+  int buf = 0;
+  double v[1] = {0.0};
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    v[0] += x[i] * y[i];
+  block_sum<1>(&sh, buf, v);
+  if (threadIdx.x == 0)
+    part[blockIdx.x] = v[0];
+}
+__global__ void __launch_bounds__(256) sum_partials_kernel(int nb, const double *part, double *out,
+                                                           int take_sqrt) {
+  __shared__ TeamShared sh;
+  int buf = 0;
+  double v[1] = {0.0};
+  for (int i = threadIdx.x; i < nb; i += blockDim.x)
+    v[0] += part[i];
+  block_sum<1>(&sh, buf, v);
+  if (threadIdx.x == 0)
+    out[0] = take_sqrt ? sqrt(v[0]) : v[0];
+}
+__global__ void axpy_kernel(int64_t n, double a, const double *x, double *y) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    y[i] += a * x[i];
+}
+__global__ void scale_kernel(int64_t n, double a, double *x) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    x[i] *= a;
+}
+__global__ void scale_by_inv_norm_kernel(int64_t n, const double *nrm, double *x) {
+  const double s = nrm[0];
+  if (!(s > 0.0))
+    return;
+  const double a = 1.0 / s;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    x[i] *= a;
+}
+__global__ void fill_kernel(int64_t n, double a, double *x) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    x[i] = a;
+}
+__global__ void to_f32_kernel(int64_t n, const double *x, float *y) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    y[i] = (float)x[i];
+}
+
+// ---- deterministic transpose: count, scan, scatter, per-row sort, gather ----
+__global__ void col_count_kernel(int64_t nnz, const int32_t *ci, int32_t *cnt) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < nnz; k += (int64_t)gridDim.x * blockDim.x)
+    atomicAdd(cnt + ci[k], 1);
+}
+// exclusive scan of cnt[0..n) into out[0..n]; single block, chunked
+__global__ void __launch_bounds__(1024) scan_kernel(int64_t n, const int32_t *cnt, int32_t *out) {
+  __shared__ int32_t s[1024];
+  __shared__ int32_t carry;
+  if (threadIdx.x == 0)
+    carry = 0;
+  __syncthreads();
+  for (int64_t base = 0; base < n; base += 1024) {
+    const int64_t i = base + threadIdx.x;
+    const int32_t v = i < n ? cnt[i] : 0;
+    s[threadIdx.x] = v;
+    __syncthreads();
+    for (int o = 1; o < 1024; o <<= 1) {
+      const int32_t t = threadIdx.x >= (unsigned)o ? s[threadIdx.x - o] : 0;
+      __syncthreads();
+      s[threadIdx.x] += t;
+      __syncthreads();
+    }
+    if (i < n)
+      out[i] = carry + s[threadIdx.x] - v;
+    __syncthreads();
+    if (threadIdx.x == 1023)
+      carry += s[1023];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    out[n] = carry;
+}
+__global__ void scatter_kernel(int64_t nnz, const int32_t *ci, int32_t *cursor, int32_t *perm) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < nnz; k += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t pos = atomicAdd(cursor + ci[k], 1);
+    perm[pos] = (int32_t)k;
+  }
+}
+// sort each transposed row's source positions ascending (warp per row):
+// rows up to 32 entries in registers (bitonic), longer rows by ranking.
+__global__ void row_sort_kernel(int64_t rows, const int32_t *rp, int32_t *perm, int32_t *tmp) {
+  const int lane = threadIdx.x & 31;
+  const int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t r = w; r < rows; r += nw) {
+    const int32_t b = rp[r], e = rp[r + 1], L = e - b;
+    if (L <= 1)
+      continue;
+    if (L <= 32) {
+      int32_t v = lane < L ? perm[b + lane] : INT32_MAX;
+      for (int k = 2; k <= 32; k <<= 1)
+        for (int j = k >> 1; j > 0; j >>= 1) {
+          const int32_t o = __shfl_xor_sync(0xffffffffu, v, j);
+          const bool up = ((lane & k) == 0);
+          const bool lower = ((lane & j) == 0);
+          v = (lower == up) ? min(v, o) : max(v, o);
+        }
+      if (lane < L)
+        perm[b + lane] = v;
+    } else {
+      for (int32_t i = lane; i < L; i += 32) {
+        const int32_t key = perm[b + i];
+        int32_t rank = 0;
+        for (int32_t j = 0; j < L; j++)
+          rank += perm[b + j] < key;
+        tmp[b + rank] = key;
+      }
+      __syncwarp();
+      for (int32_t i = lane; i < L; i += 32)
+        perm[b + i] = tmp[b + i];
+    }
+  }
+}
+__global__ void row_of_kernel(int64_t m, const int32_t *rp, int32_t *rowof) {
+  const int lane = threadIdx.x & 31;
+  const int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t r = w; r < m; r += nw)
+    for (int32_t k = rp[r] + lane; k < rp[r + 1]; k += 32)
+      rowof[k] = (int32_t)r;
+}
+__global__ void gather_t_kernel(int64_t nnz, const int32_t *perm, const int32_t *rowof, const double *v,
+                                int32_t *ciT, double *vT) {
+  for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < nnz; p += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t k = perm[p];
+    ciT[p] = rowof[k];
+    vT[p] = v[k];
+  }
+}
+
+__global__ void rng_mt_kernel(RngState *st, double *out, int64_t n) { block_mt_normals(st, out, n); }
+__global__ void rng_philox_kernel(RngState *st, double *out, int64_t n) {
+  const uint64_t key = st->philox_key, base = st->philox_ctr;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = philox_normal(key, base + (uint64_t)i);
+}
+__global__ void rng_philox_advance(RngState *st, int64_t n) { st->philox_ctr += (uint64_t)n; }
+
+static int grid_for(krans_ctx *ctx, int64_t n, int threads = 256) {
+  int64_t b = (n + threads - 1) / threads;
+  const int64_t cap = (int64_t)ctx->sms * 8;
+  if (b > cap)
+    b = cap;
+  if (b < 1)
+    b = 1;
+  return (int)b;
+}
+
+} // namespace kr
+
+using namespace kr;
+
+extern "C" {
+
+const char *krans_last_error(void) { return kr::g_last_error.c_str(); }
+const char *krans_version(void) { return "krans_b200 0.1 (sm_100a)"; }
+
+int krans_ctx_create(int device, size_t hbm_budget_bytes, krans_ctx **out) {
+  KR_CHECK_ARG(out, "krans_ctx_create: out is NULL");
+  *out = nullptr;
+  int ndev = 0;
+  KR_CUDA(cudaGetDeviceCount(&ndev));
+  KR_CHECK_ARG(device >= 0 && device < ndev, "krans_ctx_create: no such device");
+  KR_CUDA(cudaSetDevice(device));
+  auto *c = new krans_ctx();
+  c->device = device;
+  c->budget = hbm_budget_bytes;
+  cudaDeviceProp prop;
+  cudaError_t e = cudaGetDeviceProperties(&prop, device);
+  if (e != cudaSuccess) {
+    delete c;
+    return cuda_fail(e, "cudaGetDeviceProperties", __FILE__, __LINE__);
+  }
+  c->sms = prop.multiProcessorCount;
+  c->cc_major = prop.major;
+  c->cc_minor = prop.minor;
+  if (prop.major != 10) {
+    delete c;
+    set_error("krans_ctx_create: device %d is sm_%d%d; this build targets sm_100a (B200)", device,
+              prop.major, prop.minor);
+    return KRANS_ERR_RUNTIME;
+  }
+  e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess)
+    e = cudaMallocHost(&c->h_scalar, 64 * sizeof(double));
+  c->partial_blocks = c->sms * 8;
+  if (e == cudaSuccess)
+    e = cudaMalloc(&c->d_scalar, 64 * sizeof(double));
+  if (e == cudaSuccess)
+    e = cudaMalloc(&c->d_partials, (size_t)c->partial_blocks * sizeof(double));
+  if (e != cudaSuccess) {
+    int rc = cuda_fail(e, "context setup", __FILE__, __LINE__);
+    krans_ctx_destroy(c);
+    return rc;
+  }
+  *out = c;
+  return KRANS_OK;
+}
+
+int krans_ctx_destroy(krans_ctx *ctx) {
+  if (!ctx)
+    return KRANS_OK;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream)
+    cudaStreamSynchronize(ctx->stream);
+  if (ctx->h_scalar)
+    cudaFreeHost(ctx->h_scalar);
+  if (ctx->d_scalar)
+    cudaFree(ctx->d_scalar);
+  if (ctx->d_partials)
+    cudaFree(ctx->d_partials);
+  if (ctx->stream)
+    cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return KRANS_OK;
+}
+
+int krans_ctx_synchronize(krans_ctx *ctx) {
+  KR_CHECK_ARG(ctx, "NULL context");
+  KR_CUDA(cudaStreamSynchronize(ctx->stream));
+  return KRANS_OK;
+}
+
+int krans_ctx_memory_in_use(const krans_ctx *ctx, size_t *bytes) {
+  KR_CHECK_ARG(ctx && bytes, "NULL argument");
+  *bytes = ctx->in_use;
+  return KRANS_OK;
+}
+
+int krans_ctx_sm_count(const krans_ctx *ctx, int *sms) {
+  KR_CHECK_ARG(ctx && sms, "NULL argument");
+  *sms = ctx->sms;
+  return KRANS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// CSR
+// ---------------------------------------------------------------------------
+int krans_csr_create(krans_ctx *ctx, int64_t m, int64_t n, int64_t nnz, const int32_t *row_ptr,
+                     const int32_t *col_idx, const double *values, int flags, krans_mat **out) {
+  KR_CHECK_ARG(ctx && out, "krans_csr_create: NULL argument");
+  *out = nullptr;
+  KR_CHECK_ARG(m >= 0 && n >= 0 && nnz >= 0, "krans_csr_create: negative size");
+  KR_CHECK_ARG(m < INT32_MAX && n < INT32_MAX && nnz < INT32_MAX,
+               "krans_csr_create: sizes must fit 32-bit indices");
+  KR_CHECK_ARG(row_ptr && (nnz == 0 || (col_idx && values)), "krans_csr_create: NULL array");
+  KR_CHECK_ARG(row_ptr[0] == 0 && row_ptr[m] == nnz, "krans_csr_create: row_ptr[0] != 0 or row_ptr[m] != nnz");
+  for (int64_t i = 0; i < m; i++)
+    KR_CHECK_ARG(row_ptr[i] <= row_ptr[i + 1], "krans_csr_create: row_ptr not monotone");
+  for (int64_t k = 0; k < nnz; k++)
+    KR_CHECK_ARG(col_idx[k] >= 0 && col_idx[k] < n, "krans_csr_create: column index out of range");
+  if (!(flags & (KRANS_CSR_FP64 | KRANS_CSR_FP32)))
+    flags |= KRANS_CSR_FP64;
+  flags |= KRANS_CSR_FP64; // FP64 values are kept for every path (polish, residuals)
+  KR_CUDA(cudaSetDevice(ctx->device));
+  auto *A = new krans_mat();
+  A->ctx = ctx;
+  A->m = m;
+  A->n = n;
+  A->nnz = nnz;
+  const size_t sz_rp = (size_t)(m + 1) * 4, sz_rpT = (size_t)(n + 1) * 4, sz_ci = (size_t)std::max<int64_t>(nnz, 1) * 4;
+  const size_t sz_v = (size_t)std::max<int64_t>(nnz, 1) * 8, sz_v32 = (size_t)std::max<int64_t>(nnz, 1) * 4;
+  int rc = KRANS_OK;
+  auto alloc = [&](void **p, size_t b) {
+    if (rc == KRANS_OK) {
+      rc = dev_alloc(ctx, p, b);
+      if (rc == KRANS_OK)
+        A->bytes += b;
+    }
+  };
+  alloc((void **)&A->rp, sz_rp);
+  alloc((void **)&A->ci, sz_ci);
+  alloc((void **)&A->v, sz_v);
+  alloc((void **)&A->rpT, sz_rpT);
+  alloc((void **)&A->ciT, sz_ci);
+  alloc((void **)&A->vT, sz_v);
+  if (flags & KRANS_CSR_FP32) {
+    alloc((void **)&A->v32, sz_v32);
+    alloc((void **)&A->vT32, sz_v32);
+  }
+  int32_t *cnt = nullptr, *perm = nullptr, *tmp = nullptr, *rowof = nullptr;
+  alloc((void **)&cnt, sz_rpT);
+  alloc((void **)&perm, sz_ci);
+  alloc((void **)&tmp, sz_ci);
+  alloc((void **)&rowof, sz_ci);
+  if (rc != KRANS_OK) {
+    dev_free(ctx, cnt, sz_rpT);
+    dev_free(ctx, perm, sz_ci);
+    dev_free(ctx, tmp, sz_ci);
+    dev_free(ctx, rowof, sz_ci);
+    krans_csr_destroy(A);
+    return rc;
+  }
+  cudaStream_t s = ctx->stream;
+  cudaError_t e = cudaMemcpyAsync(A->rp, row_ptr, sz_rp, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess && nnz)
+    e = cudaMemcpyAsync(A->ci, col_idx, (size_t)nnz * 4, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess && nnz)
+    e = cudaMemcpyAsync(A->v, values, (size_t)nnz * 8, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess)
+    e = cudaMemsetAsync(cnt, 0, sz_rpT, s);
+  if (e == cudaSuccess && nnz) {
+    const int g = grid_for(ctx, nnz);
+    col_count_kernel<<<g, 256, 0, s>>>(nnz, A->ci, cnt);
+    scan_kernel<<<1, 1024, 0, s>>>(n, cnt, A->rpT);
+    e = cudaMemcpyAsync(cnt, A->rpT, (size_t)n * 4, cudaMemcpyDeviceToDevice, s);
+    scatter_kernel<<<g, 256, 0, s>>>(nnz, A->ci, cnt, perm);
+    row_sort_kernel<<<grid_for(ctx, n * 32), 256, 0, s>>>(n, A->rpT, perm, tmp);
+    row_of_kernel<<<grid_for(ctx, m * 32), 256, 0, s>>>(m, A->rp, rowof);
+    gather_t_kernel<<<g, 256, 0, s>>>(nnz, perm, rowof, A->v, A->ciT, A->vT);
+    if (flags & KRANS_CSR_FP32) {
+      to_f32_kernel<<<g, 256, 0, s>>>(nnz, A->v, A->v32);
+      to_f32_kernel<<<g, 256, 0, s>>>(nnz, A->vT, A->vT32);
+    }
+  } else if (e == cudaSuccess) {
+    e = cudaMemsetAsync(A->rpT, 0, sz_rpT, s);
+  }
+  if (e == cudaSuccess)
+    e = cudaGetLastError();
+  if (e == cudaSuccess)
+    e = cudaStreamSynchronize(s);
+  dev_free(ctx, cnt, sz_rpT);
+  dev_free(ctx, perm, sz_ci);
+  dev_free(ctx, tmp, sz_ci);
+  dev_free(ctx, rowof, sz_ci);
+  if (e != cudaSuccess) {
+    rc = cuda_fail(e, "krans_csr_create", __FILE__, __LINE__);
+    krans_csr_destroy(A);
+    return rc;
+  }
+  A->lanes = pick_lanes(m, nnz);
+  A->lanesT = pick_lanes(n, nnz);
+  *out = A;
+  return KRANS_OK;
+}
+
+int krans_csr_destroy(krans_mat *A) {
+  if (!A)
+    return KRANS_OK;
+  krans_ctx *c = A->ctx;
+  const size_t sz_rp = (size_t)(A->m + 1) * 4, sz_rpT = (size_t)(A->n + 1) * 4;
+  const size_t sz_ci = (size_t)std::max<int64_t>(A->nnz, 1) * 4, sz_v = (size_t)std::max<int64_t>(A->nnz, 1) * 8;
+  dev_free(c, A->rp, sz_rp);
+  dev_free(c, A->ci, sz_ci);
+  dev_free(c, A->v, sz_v);
+  dev_free(c, A->rpT, sz_rpT);
+  dev_free(c, A->ciT, sz_ci);
+  dev_free(c, A->vT, sz_v);
+  dev_free(c, A->v32, sz_ci);
+  dev_free(c, A->vT32, sz_ci);
+  delete A;
+  return KRANS_OK;
+}
+
+int krans_csr_dims(const krans_mat *A, int64_t *m, int64_t *n, int64_t *nnz) {
+  KR_CHECK_ARG(A, "NULL matrix");
+  if (m)
+    *m = A->m;
+  if (n)
+    *n = A->n;
+  if (nnz)
+    *nnz = A->nnz;
+  return KRANS_OK;
+}
+
+int krans_csr_device_arrays(const krans_mat *A, int trans, const int32_t **row_ptr,
+                            const int32_t **col_idx, const double **values, const float **values32) {
+  KR_CHECK_ARG(A, "NULL matrix");
+  if (row_ptr)
+    *row_ptr = trans ? A->rpT : A->rp;
+  if (col_idx)
+    *col_idx = trans ? A->ciT : A->ci;
+  if (values)
+    *values = trans ? A->vT : A->v;
+  if (values32)
+    *values32 = trans ? A->vT32 : A->v32;
+  return KRANS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// vectors
+// ---------------------------------------------------------------------------
+int krans_vec_create(krans_ctx *ctx, int64_t n, krans_vec **out) {
+  KR_CHECK_ARG(ctx && out, "krans_vec_create: NULL argument");
+  KR_CHECK_ARG(n >= 0, "krans_vec_create: negative size");
+  *out = nullptr;
+  auto *v = new krans_vec();
+  v->ctx = ctx;
+  v->n = n;
+  int rc = dev_alloc(ctx, (void **)&v->d, (size_t)std::max<int64_t>(n, 1) * 8);
+  if (rc != KRANS_OK) {
+    delete v;
+    return rc;
+  }
+  cudaError_t e = cudaMemsetAsync(v->d, 0, (size_t)std::max<int64_t>(n, 1) * 8, ctx->stream);
+  if (e != cudaSuccess) {
+    dev_free(ctx, v->d, (size_t)std::max<int64_t>(n, 1) * 8);
+    delete v;
+    return cuda_fail(e, "cudaMemsetAsync", __FILE__, __LINE__);
+  }
+  *out = v;
+  return KRANS_OK;
+}
+
+int krans_vec_destroy(krans_vec *v) {
+  if (!v)
+    return KRANS_OK;
+  dev_free(v->ctx, v->d, (size_t)std::max<int64_t>(v->n, 1) * 8);
+  delete v;
+  return KRANS_OK;
+}
+
+int krans_vec_size(const krans_vec *v, int64_t *n) {
+  KR_CHECK_ARG(v && n, "NULL argument");
+  *n = v->n;
+  return KRANS_OK;
+}
+
+int krans_vec_device_ptr(krans_vec *v, double **dptr) {
+  KR_CHECK_ARG(v && dptr, "NULL argument");
+  *dptr = v->d;
+  return KRANS_OK;
+}
+
+int krans_vec_upload(krans_vec *v, const double *host, int64_t n) {
+  KR_CHECK_ARG(v && (host || n == 0), "NULL argument");
+  KR_CHECK_ARG(n == v->n, "krans_vec_upload: size mismatch");
+  if (n)
+    KR_CUDA(cudaMemcpyAsync(v->d, host, (size_t)n * 8, cudaMemcpyHostToDevice, v->ctx->stream));
+  KR_CUDA(cudaStreamSynchronize(v->ctx->stream));
+  return KRANS_OK;
+}
+
+int krans_vec_download(const krans_vec *v, double *host, int64_t n) {
+  KR_CHECK_ARG(v && (host || n == 0), "NULL argument");
+  KR_CHECK_ARG(n == v->n, "krans_vec_download: size mismatch");
+  if (n)
+    KR_CUDA(cudaMemcpyAsync(host, v->d, (size_t)n * 8, cudaMemcpyDeviceToHost, v->ctx->stream));
+  KR_CUDA(cudaStreamSynchronize(v->ctx->stream));
+  return KRANS_OK;
+}
+
+static int reduce_to_host(krans_ctx *c, int64_t n, const double *x, const double *y, int take_sqrt,
+                          double *out) {
+  const int g = std::min<int>(grid_for(c, n), c->partial_blocks);
+  dot_partial_kernel<<<g, 256, 0, c->stream>>>(n, x, y, c->d_partials);
+  sum_partials_kernel<<<1, 256, 0, c->stream>>>(g, c->d_partials, c->d_scalar, take_sqrt);
+  KR_CUDA(cudaGetLastError());
+  KR_CUDA(cudaMemcpyAsync(c->h_scalar, c->d_scalar, 8, cudaMemcpyDeviceToHost, c->stream));
+  KR_CUDA(cudaStreamSynchronize(c->stream));
+  *out = c->h_scalar[0];
+  return KRANS_OK;
+}
+
+int krans_vec_dot(const krans_vec *x, const krans_vec *y, double *out) {
+  KR_CHECK_ARG(x && y && out, "NULL argument");
+  KR_CHECK_ARG(x->n == y->n, "krans_vec_dot: size mismatch");
+  return reduce_to_host(x->ctx, x->n, x->d, y->d, 0, out);
+}
+
+int krans_vec_nrm2(const krans_vec *v, double *out) {
+  KR_CHECK_ARG(v && out, "NULL argument");
+  return reduce_to_host(v->ctx, v->n, v->d, v->d, 1, out);
+}
+
+int krans_vec_axpy(krans_vec *y, double alpha, const krans_vec *x) {
+  KR_CHECK_ARG(x && y, "NULL argument");
+  KR_CHECK_ARG(x->n == y->n, "krans_vec_axpy: size mismatch");
+  axpy_kernel<<<grid_for(y->ctx, y->n), 256, 0, y->ctx->stream>>>(y->n, alpha, x->d, y->d);
+  KR_CUDA(cudaGetLastError());
+  return KRANS_OK;
+}
+
+int krans_vec_scale(krans_vec *v, double alpha) {
+  KR_CHECK_ARG(v, "NULL argument");
+  scale_kernel<<<grid_for(v->ctx, v->n), 256, 0, v->ctx->stream>>>(v->n, alpha, v->d);
+  KR_CUDA(cudaGetLastError());
+  return KRANS_OK;
+}
+
+int krans_vec_normalize(krans_vec *v) {
+  KR_CHECK_ARG(v, "NULL argument");
+  krans_ctx *c = v->ctx;
+  const int g = std::min<int>(grid_for(c, v->n), c->partial_blocks);
+  dot_partial_kernel<<<g, 256, 0, c->stream>>>(v->n, v->d, v->d, c->d_partials);
+  sum_partials_kernel<<<1, 256, 0, c->stream>>>(g, c->d_partials, c->d_scalar, 1);
+  scale_by_inv_norm_kernel<<<grid_for(c, v->n), 256, 0, c->stream>>>(v->n, c->d_scalar, v->d);
+  KR_CUDA(cudaGetLastError());
+  return KRANS_OK;
+}
+
+int krans_vec_fill(krans_vec *v, double value) {
+  KR_CHECK_ARG(v, "NULL argument");
+  fill_kernel<<<grid_for(v->ctx, v->n), 256, 0, v->ctx->stream>>>(v->n, value, v->d);
+  KR_CUDA(cudaGetLastError());
+  return KRANS_OK;
+}
+
+int krans_vec_copy(krans_vec *dst, const krans_vec *src) {
+  KR_CHECK_ARG(dst && src, "NULL argument");
+  KR_CHECK_ARG(dst->n == src->n, "krans_vec_copy: size mismatch");
+  if (dst->n)
+    KR_CUDA(cudaMemcpyAsync(dst->d, src->d, (size_t)dst->n * 8, cudaMemcpyDeviceToDevice, dst->ctx->stream));
+  return KRANS_OK;
+}
+
+int krans_vec_clone(const krans_vec *src, krans_vec **out) {
+  KR_CHECK_ARG(src && out, "NULL argument");
+  int rc = krans_vec_create(src->ctx, src->n, out);
+  if (rc != KRANS_OK)
+    return rc;
+  return krans_vec_copy(*out, src);
+}
+
+int krans_spmv_ex(const krans_mat *A, int trans, int precision, const krans_vec *x, krans_vec *y) {
+  KR_CHECK_ARG(A && x && y, "krans_spmv: NULL argument");
+  const int64_t rows = trans ? A->n : A->m, cols = trans ? A->m : A->n;
+  KR_CHECK_ARG(x->n == cols && y->n == rows, "krans_spmv: size mismatch");
+  krans_ctx *c = A->ctx;
+  const int32_t *rp = trans ? A->rpT : A->rp, *ci = trans ? A->ciT : A->ci;
+  const int lanes = trans ? A->lanesT : A->lanes;
+  const int g = grid_for(c, rows * lanes);
+  if (precision == KRANS_PREC_MIXED) {
+    KR_CHECK_ARG(A->v32, "krans_spmv: matrix has no FP32 values (create with KRANS_CSR_FP32)");
+    spmv_kernel<float, double, double><<<g, 256, 0, c->stream>>>(rows, rp, ci, trans ? A->vT32 : A->v32,
+                                                                 x->d, y->d, lanes);
+  } else {
+    spmv_kernel<double, double, double><<<g, 256, 0, c->stream>>>(rows, rp, ci, trans ? A->vT : A->v, x->d,
+                                                                  y->d, lanes);
+  }
+  KR_CUDA(cudaGetLastError());
+  return KRANS_OK;
+}
+
+int krans_spmv(const krans_mat *A, int trans, const krans_vec *x, krans_vec *y) {
+  return krans_spmv_ex(A, trans, KRANS_PREC_FP64, x, y);
+}
+
+// ---------------------------------------------------------------------------
+// RNG
+// ---------------------------------------------------------------------------
+static void mt_seed_host(RngState &s, uint32_t seed) {
+  s.mt[0] = seed;
+  for (int i = 1; i < 624; i++)
+    s.mt[i] = 1812433253u * (s.mt[i - 1] ^ (s.mt[i - 1] >> 30)) + (uint32_t)i;
+  s.idx = 624;
+  s.has_saved = 0;
+  s.saved = 0.0;
+}
+
+int krans_rng_create(krans_ctx *ctx, uint32_t seed, int mode, krans_rng **out) {
+  KR_CHECK_ARG(ctx && out, "krans_rng_create: NULL argument");
+  KR_CHECK_ARG(mode == KRANS_RNG_MT19937 || mode == KRANS_RNG_PHILOX, "krans_rng_create: bad mode");
+  *out = nullptr;
+  if (seed == 0)
+    seed = std::random_device{}();
+  RngState h;
+  memset(&h, 0, sizeof h);
+  mt_seed_host(h, seed);
+  h.philox_key = ((uint64_t)seed << 32) ^ 0x9E3779B97F4A7C15ull;
+  h.philox_ctr = 0;
+  h.mode = mode;
+  auto *r = new krans_rng();
+  r->ctx = ctx;
+  r->seed = seed;
+  r->mode = mode;
+  int rc = dev_alloc(ctx, (void **)&r->d, sizeof(RngState));
+  if (rc != KRANS_OK) {
+    delete r;
+    return rc;
+  }
+  cudaError_t e = cudaMemcpyAsync(r->d, &h, sizeof h, cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess)
+    e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) {
+    krans_rng_destroy(r);
+    return cuda_fail(e, "rng upload", __FILE__, __LINE__);
+  }
+  *out = r;
+  return KRANS_OK;
+}
+
+int krans_rng_destroy(krans_rng *r) {
+  if (!r)
+    return KRANS_OK;
+  dev_free(r->ctx, r->d, sizeof(RngState));
+  delete r;
+  return KRANS_OK;
+}
+
+int krans_rng_seed(const krans_rng *r, uint32_t *seed) {
+  KR_CHECK_ARG(r && seed, "NULL argument");
+  *seed = r->seed;
+  return KRANS_OK;
+}
+
+int krans_rng_normal(krans_rng *r, krans_vec *out) {
+  KR_CHECK_ARG(r && out, "krans_rng_normal: NULL argument");
+  krans_ctx *c = r->ctx;
+  if (r->mode == KRANS_RNG_PHILOX) {
+    rng_philox_kernel<<<grid_for(c, out->n), 256, 0, c->stream>>>(r->d, out->d, out->n);
+    rng_philox_advance<<<1, 1, 0, c->stream>>>(r->d, out->n);
+  } else {
+    rng_mt_kernel<<<1, 256, 0, c->stream>>>(r->d, out->d, out->n);
+  }
+  KR_CUDA(cudaGetLastError());
+  return KRANS_OK;
+}
+
+int krans_cyclic_opts_init(krans_cyclic_opts *o) {
+  KR_CHECK_ARG(o, "NULL argument");
+  memset(o, 0, sizeof *o);
+  o->k = 1;
+  o->ncv = 48;
+  o->max_restarts = 80;
+  o->tol_abs = 1e-12;
+  o->tol_rel = 1e-10;
+  o->reorth = 2;
+  o->use_harmonic = 1;
+  o->target_tau = 0.0;
+  o->nullity_known = -1;
+  o->rank_known = -1;
+  o->cg_maxit = 80;
+  o->cg_rel_tol = 1e-10;
+  o->cg_breakdown_tol = 1e-30;
+  o->projector_passes = 1;
+  o->grad_max_iters = 3000;
+  o->frob_samples = 4;
+  o->prescreen_factor = 0.8;
+  o->stagnation_restarts = 30;
+  o->return_left_space = 0;
+  o->verbose = 0;
+  o->precision = KRANS_PREC_FP64;
+  o->team = KRANS_TEAM_AUTO;
+  return KRANS_OK;
+}
+
+int krans_lobpcg_opts_init(krans_lobpcg_opts *o) {
+  KR_CHECK_ARG(o, "NULL argument");
+  memset(o, 0, sizeof *o);
+  o->nev = 1;
+  o->block_size = 0;
+  o->max_iters = 1000;
+  o->tol_abs = 1e-12;
+  o->tol_rel = 1e-10;
+  o->soft_locking = 1;
+  o->restart = 0.9;
+  o->gs_tol = 1e-14;
+  o->gs_reorth = 1;
+  o->frob_samples = 4;
+  o->max_tiny_dim = 0;
+  o->nullity_known = -1;
+  o->rank_known = -1;
+  o->progress_every = 100;
+  o->precision = KRANS_PREC_FP64;
+  o->team = KRANS_TEAM_AUTO;
+  return KRANS_OK;
+}
+
+} // extern "C"

@@ -1,0 +1,723 @@
+// Cyclic Lanczos (Golub-Kahan) null-space solver on the device.
+//
+// Restates find_right_nullspace of the reference
+// (src/Solvers/CyclicLanczosSolver.cpp:291-616) as team code: the whole
+// restart / candidate / polish control flow runs on the GPU, with every
+// decision taken from team-wide reductions so all threads follow one path.
+// Differences that only change rounding:
+//  - reorthogonalisation is block classical Gram-Schmidt, two passes (CGS2)
+//    instead of vector-by-vector MGS (CyclicLanczosSolver.cpp:26-33,399-407);
+//  - dot products are fixed-tree reductions instead of sequential sums;
+//  - the refined-extraction SVD uses the even/odd decoupling of Tbar when
+//    tau = 0 (all alpha are zero, so right singular vectors live on either
+//    the [0;y] or the [x;0] Lanczos vectors; only the [0;y] ones can be
+//    candidates, CyclicLanczosSolver.cpp:474-480).
+// Precision: KT is the storage type of the Krylov vectors and of the
+// SpMV in the Golub-Kahan recurrence (double: plain FP64 path; float: mixed
+// path with FP32 SpMV and FP32 accumulation). Reorthogonalisation inner
+// products, the projected SVD, the candidate vectors, the CG projector polish
+// and the acceptance residuals are FP64 with FP64 matrix values in both.
+#pragma once
+
+#include "kr_dense.cuh"
+#include "kr_device.cuh"
+
+namespace kr {
+
+struct CsrView {
+  int64_t rows, cols, nnz;
+  const int32_t *rp, *ci;
+  const double *v64;
+  const float *v32;
+  int lanes; // threads per row in the SpMV
+};
+
+struct CyclicDevResult {
+  int64_t n_found;
+  int64_t restarts, krylov_steps_total, cg_solves, cg_maxit_hits, spmv, spmvT;
+  double frob, bytes;
+  int32_t converged;
+  int32_t status;
+};
+
+struct CyclicDesc {
+  CsrView F, B; // F: the run's operator (rows m, cols n); B: its transpose
+  krans_cyclic_opts o;
+  int64_t k_target, ncv;
+  int32_t trans_run; // 1 for the left-space run (counts swap)
+  RngState *rng;
+  const double *initial_right; // n doubles or nullptr
+  double *basis;               // k_target x ldn (output, row i = vector i)
+  void *Y, *X, *wx, *wy;       // KT storage
+  double *y0, *v, *vp, *best_v, *tn; // n-vectors
+  double *tmv, *wm, *r, *p, *Ap;     // m-vectors
+  double *alpha, *beta;              // ncv + 2
+  double *Tb, *Vt, *sv;              // tiny problem
+  int32_t *ord;
+  double *eig_cs;
+  int32_t *eig_pq, *eig_ord;
+  int64_t ldn, ldm, ldb, cap; // ldb: stride of the basis rows
+  int32_t *status;
+  CyclicDevResult *res;
+  GridBarrierState *gb;
+  double *gpart;
+};
+
+// counters kept identically by every thread (uniform control flow)
+struct Counters {
+  int64_t spmv = 0, spmvT = 0, cg_solves = 0, cg_maxit_hits = 0, steps = 0, restarts = 0;
+  double bytes = 0.0;
+};
+
+template <class Team, class KT> struct CyclicSolver {
+  Team &tm;
+  const CyclicDesc &d;
+  Counters c;
+  int64_t m, n, nb = 0;
+  double frob = 0.0;
+
+  KR_DEV CyclicSolver(Team &t, const CyclicDesc &dd) : tm(t), d(dd) {
+    m = d.F.rows;
+    n = d.F.cols;
+  }
+
+  KR_DEV void count_F() {
+    if (d.trans_run)
+      c.spmvT++;
+    else
+      c.spmv++;
+  }
+  KR_DEV void count_B() {
+    if (d.trans_run)
+      c.spmv++;
+    else
+      c.spmvT++;
+  }
+
+  // y = F x (FP64)
+  KR_DEV void mulF(const double *x, double *y) {
+    team_spmv(tm, d.F.rows, d.F.rp, d.F.ci, d.F.v64, x, d.F.lanes,
+              [&](int64_t i, double s) { y[i] = s; });
+    count_F();
+    c.bytes += spmv_bytes(d.F.rows, d.F.cols, d.F.nnz, 8, 8, 8);
+    tm.sync();
+  }
+  KR_DEV void mulB(const double *x, double *y) {
+    team_spmv(tm, d.B.rows, d.B.rp, d.B.ci, d.B.v64, x, d.B.lanes,
+              [&](int64_t i, double s) { y[i] = s; });
+    count_B();
+    c.bytes += spmv_bytes(d.B.rows, d.B.cols, d.B.nnz, 8, 8, 8);
+    tm.sync();
+  }
+  // ||F x|| with y = F x stored (fused norm)
+  KR_DEV double mulF_norm(const double *x, double *y) {
+    double s2 = 0.0;
+    team_spmv(tm, d.F.rows, d.F.rp, d.F.ci, d.F.v64, x, d.F.lanes, [&](int64_t i, double s) {
+      y[i] = s;
+      s2 += s * s;
+    });
+    count_F();
+    c.bytes += spmv_bytes(d.F.rows, d.F.cols, d.F.nnz, 8, 8, 8);
+    return sqrt(tm.sum1(s2)); // the reduction's barrier also publishes y
+  }
+
+  KR_DEV double nrm2(int64_t len, const double *x) {
+    c.bytes += 8.0 * len;
+    return team_nrm2(tm, len, x);
+  }
+  KR_DEV void scale(int64_t len, double a, double *x) {
+    team_for(tm, len, [&](int64_t i) { x[i] *= a; });
+    c.bytes += 16.0 * len;
+    tm.sync();
+  }
+  KR_DEV void copy(int64_t len, const double *s, double *dd) {
+    team_for(tm, len, [&](int64_t i) { dd[i] = s[i]; });
+    c.bytes += 16.0 * len;
+    tm.sync();
+  }
+  KR_DEV void random(double *out) {
+    team_random_normal(tm, d.rng, out, n);
+    c.bytes += 8.0 * n;
+  }
+
+  // two classical Gram-Schmidt passes against the accepted basis (double)
+  KR_DEV void gs2_basis(double *v) {
+    if (nb == 0)
+      return;
+    for (int pass = 0; pass < 2; pass++) {
+      team_multidot(tm, n, d.basis, d.ldb, (int)nb, v);
+      team_multi_axpy(tm, n, d.basis, d.ldb, (int)nb, tm.sh->h, v);
+      c.bytes += 2.0 * (nb + 1) * 8.0 * n + 8.0 * n;
+      tm.sync();
+    }
+  }
+  // one CGS pass of w (len) against ns stored vectors S (type TS)
+  template <class TS, class TW> KR_DEV void cgs_pass(int64_t len, const TS *S, int64_t ld, int ns, TW *w) {
+    if (ns == 0)
+      return;
+    team_multidot(tm, len, S, ld, ns, w);
+    team_multi_axpy(tm, len, S, ld, ns, tm.sh->h, w);
+    c.bytes += (double)(2 * ns + 3) * sizeof(TS) * len;
+    tm.sync();
+  }
+
+  KR_DEV double fro_est() {
+    const int samples = d.o.frob_samples > 1 ? d.o.frob_samples : 1;
+    double sum2 = 0.0;
+    for (int s = 0; s < samples; s++) {
+      random(d.tn);
+      const double nr = mulF_norm(d.tn, d.tmv);
+      sum2 += nr * nr;
+    }
+    return sqrt(sum2 / (double)samples);
+  }
+
+  // CG on (F F^T) w = rhs (CyclicLanczosSolver.cpp:48-113), no preconditioner.
+  KR_DEV int64_t cg(const double *rhs, double *w, int64_t maxit, double rel_tol, double bd_tol,
+                    double *rnorm_out) {
+    double *r = d.r, *p = d.p, *Ap = d.Ap, *tn = d.tn;
+    double rr = 0.0;
+    team_for(tm, m, [&](int64_t i) {
+      const double x = rhs[i];
+      w[i] = 0.0;
+      r[i] = x;
+      p[i] = x;
+      rr += x * x;
+    });
+    rr = tm.sum1(rr);
+    c.bytes += 32.0 * m;
+    const double rhsn = sqrt(rr > 0.0 ? rr : 0.0);
+    *rnorm_out = rhsn;
+    if (!(rhsn > 0.0) || !isfinite(rhsn))
+      return 0;
+    double rz = rr; // z = r without a preconditioner
+    if (!(rz > 0.0) || !isfinite(rz))
+      return 0;
+    double rnorm = sqrt(rz);
+    const double tol = fmax(rel_tol * rnorm, 1e-30);
+    *rnorm_out = rnorm;
+    if (rnorm <= tol)
+      return 0;
+    int64_t k = 0;
+    for (; k < maxit && tm.ok(); ++k) {
+      mulB(p, tn);
+      double pap = 0.0;
+      team_spmv(tm, d.F.rows, d.F.rp, d.F.ci, d.F.v64, tn, d.F.lanes, [&](int64_t i, double s) {
+        Ap[i] = s;
+        pap += p[i] * s;
+      });
+      count_F();
+      c.bytes += spmv_bytes(d.F.rows, d.F.cols, d.F.nnz, 8, 8, 8) + 8.0 * m;
+      pap = tm.sum1(pap);
+      if (!isfinite(pap) || fabs(pap) <= bd_tol)
+        break;
+      const double alpha = rz / pap;
+      double rzn = 0.0;
+      team_for(tm, m, [&](int64_t i) {
+        w[i] += alpha * p[i];
+        const double ri = r[i] - alpha * Ap[i];
+        r[i] = ri;
+        rzn += ri * ri;
+      });
+      rzn = tm.sum1(rzn);
+      c.bytes += 40.0 * m;
+      if (!isfinite(rzn))
+        break;
+      rnorm = sqrt(rzn > 0.0 ? rzn : 0.0);
+      if (rnorm <= tol) {
+        ++k;
+        break;
+      }
+      const double beta = rzn / fmax(1e-300, rz);
+      rz = rzn;
+      team_for(tm, m, [&](int64_t i) { p[i] = p[i] * beta + r[i]; });
+      c.bytes += 24.0 * m;
+      tm.sync();
+    }
+    *rnorm_out = rnorm;
+    return k;
+  }
+
+  // try_project_random_to_nullspace (CyclicLanczosSolver.cpp:140-214)
+  KR_DEV bool try_project_random(double accept) {
+    double *v = d.v, *tmv = d.tmv, *wm = d.wm, *tn = d.tn;
+    random(v);
+    // single GS pass vs basis
+    if (nb > 0) {
+      team_multidot(tm, n, d.basis, d.ldb, (int)nb, v);
+      team_multi_axpy(tm, n, d.basis, d.ldb, (int)nb, tm.sh->h, v);
+      tm.sync();
+    }
+    double nv = nrm2(n, v);
+    if (nv < 1e-14)
+      return false;
+    scale(n, 1.0 / nv, v);
+    const double tnorm = mulF_norm(v, tmv);
+    double rn;
+    const int64_t its = cg(tmv, wm, 500, 1e-12, 1e-30, &rn);
+    if (its > 0 || rn < tnorm) {
+      mulB(wm, tn);
+      team_for(tm, n, [&](int64_t i) { v[i] -= tn[i]; });
+      tm.sync();
+    }
+    if (nb > 0) {
+      team_multidot(tm, n, d.basis, d.ldb, (int)nb, v);
+      team_multi_axpy(tm, n, d.basis, d.ldb, (int)nb, tm.sh->h, v);
+      tm.sync();
+    }
+    nv = nrm2(n, v);
+    if (nv >= 1e-14)
+      scale(n, 1.0 / nv, v);
+    double res = mulF_norm(v, tmv);
+    if (res > accept) {
+      const double fn = fro_est();
+      const double L2 = fmax(1e-30, fn * fn);
+      const double tau = 0.9 / L2;
+      for (int it = 0; it < d.o.grad_max_iters && res > accept && tm.ok(); ++it) {
+        mulF(v, tmv);
+        mulB(tmv, tn);
+        team_for(tm, n, [&](int64_t i) { v[i] -= tau * tn[i]; });
+        tm.sync();
+        if (nb > 0) {
+          team_multidot(tm, n, d.basis, d.ldb, (int)nb, v);
+          team_multi_axpy(tm, n, d.basis, d.ldb, (int)nb, tm.sh->h, v);
+          tm.sync();
+        }
+        nv = nrm2(n, v);
+        if (nv < 1e-14)
+          return false;
+        scale(n, 1.0 / nv, v);
+        res = mulF_norm(v, tmv);
+      }
+    }
+    if (res <= accept) {
+      copy(n, v, d.basis + nb * d.ldb);
+      nb++;
+      return true;
+    }
+    return false;
+  }
+
+  // Build and solve the projected problem on the leader block. Writes the
+  // candidate coefficient matrix (over the Y vectors) into d.Vt, their
+  // ordering into d.ord; returns the number of candidates (uniform).
+  KR_DEV int tiny_problem(int l, double beta_last, int ny) {
+    const double tau = d.o.target_tau;
+    const bool harmonic = d.o.use_harmonic != 0;
+    const bool split = harmonic && tau == 0.0;
+    int ncand = 0;
+    if (split)
+      ncand = (l + 1) / 2;
+    else
+      ncand = l;
+    if (tm.lead_cta()) {
+      double *Tb = d.Tb, *Vt = d.Vt, *sv = d.sv;
+      int32_t *ord = d.ord;
+      if (split) {
+        // even columns of Tbar: column i=2t has beta[i-1] at row i-1 and
+        // beta[i] (or beta_last for i = l-1) at row i+1
+        const int ce = ncand, r = l + 1;
+        for (int e = threadIdx.x; e < r * ce; e += blockDim.x) {
+          const int t = e / r, row = e % r, i = 2 * t;
+          double val = 0.0;
+          if (row == i - 1)
+            val = d.beta[i - 1];
+          else if (row == i + 1)
+            val = (i + 1 < l) ? d.beta[i] : beta_last;
+          Tb[e] = val;
+        }
+        __syncthreads();
+        block_jacobi_svd(r, ce, Tb, r, Vt, sv);
+        // ascending, ties by index
+        for (int i = threadIdx.x; i < ce; i += blockDim.x) {
+          int rank = 0;
+          for (int j = 0; j < ce; j++)
+            if (sv[j] < sv[i] || (sv[j] == sv[i] && j < i))
+              rank++;
+          ord[rank] = i;
+        }
+        __syncthreads();
+      } else if (harmonic) {
+        const int r = l + 1;
+        for (int e = threadIdx.x; e < r * l; e += blockDim.x) {
+          const int j = e / r, i = e % r;
+          double val = 0.0;
+          if (i < l) {
+            if (i == j)
+              val = d.alpha[i] - tau;
+            else if (j == i + 1 && i + 1 < l)
+              val = d.beta[i];
+            else if (i == j + 1 && j + 1 < l)
+              val = d.beta[j];
+          } else if (j == l - 1) {
+            val = beta_last;
+          }
+          Tb[e] = val;
+        }
+        __syncthreads();
+        block_jacobi_svd(r, l, Tb, r, d.eig_cs + 0, sv); // V into eig_cs scratch
+        // move V (l x l) into Vt keeping only even rows as Y coefficients
+        for (int e = threadIdx.x; e < l * l; e += blockDim.x)
+          Vt[e] = d.eig_cs[e];
+        __syncthreads();
+        for (int i = threadIdx.x; i < l; i += blockDim.x) {
+          int rank = 0;
+          for (int j = 0; j < l; j++)
+            if (sv[j] < sv[i] || (sv[j] == sv[i] && j < i))
+              rank++;
+          ord[rank] = i;
+        }
+        __syncthreads();
+      } else {
+        for (int e = threadIdx.x; e < l * l; e += blockDim.x) {
+          const int j = e / l, i = e % l;
+          double val = 0.0;
+          if (i == j)
+            val = d.alpha[i];
+          else if (j == i + 1)
+            val = d.beta[i];
+          else if (i == j + 1)
+            val = d.beta[j];
+          Tb[e] = val;
+        }
+        __syncthreads();
+        block_jacobi_eig(l, Tb, sv, Vt, d.eig_cs, d.eig_pq, d.eig_ord);
+        // already ascending by value; reorder by |lambda - tau| (stable)
+        for (int i = threadIdx.x; i < l; i += blockDim.x) {
+          const double ki = fabs(sv[i] - tau);
+          int rank = 0;
+          for (int j = 0; j < l; j++) {
+            const double kj = fabs(sv[j] - tau);
+            if (kj < ki || (kj == ki && j < i))
+              rank++;
+          }
+          ord[rank] = i;
+        }
+        __syncthreads();
+      }
+      // finiteness flag
+      __shared__ int s_bad;
+      if (threadIdx.x == 0)
+        s_bad = 0;
+      __syncthreads();
+      const int nv = split ? ncand * ncand : l * l;
+      for (int e = threadIdx.x; e < nv; e += blockDim.x)
+        if (!isfinite(Vt[e]))
+          s_bad = 1;
+      for (int e = threadIdx.x; e < ncand; e += blockDim.x)
+        if (!isfinite(sv[e]))
+          s_bad = 1;
+      __syncthreads();
+      if (threadIdx.x == 0)
+        d.ord[ncand] = s_bad; // flag slot after the ordering
+    }
+    tm.publish();
+    const int bad = *(volatile int32_t *)&d.ord[ncand];
+    (void)ny;
+    return bad ? -1 : ncand;
+  }
+
+  // coefficient of Y[t] in candidate column jb
+  KR_DEV double coef(bool split, int l, int jb, int t) const {
+    if (split)
+      return *(volatile double *)&d.Vt[(size_t)jb * ((l + 1) / 2) + t];
+    return *(volatile double *)&d.Vt[(size_t)jb * l + 2 * t];
+  }
+
+  KR_DEV void run() {
+    const krans_cyclic_opts &o = d.o;
+    KT *Y = (KT *)d.Y, *X = (KT *)d.X, *wx = (KT *)d.wx, *wy = (KT *)d.wy;
+    const int64_t ldn = d.ldn, ldm = d.ldm;
+    const int64_t k_target = d.k_target, ncv = d.ncv;
+    bool converged = false;
+
+    frob = fro_est();
+    const double fmx = fmax(1.0, frob);
+    const double accept = fmax(o.tol_abs, o.tol_rel * fmx);
+    const double prescreen = fmax(0.0, o.prescreen_factor) * fmx;
+
+    double *y0 = d.y0, *v = d.v, *vp = d.vp, *best_v = d.best_v, *tn = d.tn;
+    double *tmv = d.tmv, *wm = d.wm;
+    if (d.initial_right)
+      copy(n, d.initial_right, y0);
+    else
+      random(y0);
+
+    int64_t rsa = 0;
+    for (int64_t restart = 0; restart < o.max_restarts && tm.ok(); ++restart) {
+      c.restarts = restart;
+      gs2_basis(y0);
+      double ny = nrm2(n, y0);
+      if (!isfinite(ny) || ny < 1e-14) {
+        random(y0);
+        gs2_basis(y0);
+        ny = nrm2(n, y0);
+        if (!(ny >= 1e-14))
+          break;
+      }
+      {
+        const double s = 1.0 / ny;
+        team_for(tm, n, [&](int64_t i) {
+          const double t = y0[i] * s;
+          y0[i] = t;
+          Y[i] = (KT)t;
+        });
+        c.bytes += (8.0 + 8.0 + sizeof(KT)) * n;
+        tm.sync();
+      }
+      int nY = 1, nX = 0, na = 0, nbeta = 0;
+      int64_t local_steps = 0;
+      double beta_last = 0.0, beta_prev = 0.0; // beta_prev: uniform register copy
+      for (int64_t j = 0; j < ncv && tm.ok(); ++j) {
+        const bool from_y = nY > nX;
+        if (from_y) {
+          const KT *yj = Y + (int64_t)(nY - 1) * ldn;
+          const KT *xp = X + (int64_t)(nX > 0 ? nX - 1 : 0) * ldm;
+          const KT bp = (KT)(nbeta > 0 ? beta_prev : 0.0);
+          const bool sub = nbeta > 0;
+          if constexpr (sizeof(KT) == 8) {
+            team_spmv(tm, d.F.rows, d.F.rp, d.F.ci, d.F.v64, yj, d.F.lanes,
+                      [&](int64_t i, double s) { wx[i] = sub ? (KT)(s - (double)bp * (double)xp[i]) : (KT)s; });
+          } else {
+            team_spmv(tm, d.F.rows, d.F.rp, d.F.ci, d.F.v32, yj, d.F.lanes,
+                      [&](int64_t i, float s) { wx[i] = sub ? (KT)(s - (float)bp * (float)xp[i]) : (KT)s; });
+          }
+          count_F();
+          c.bytes += spmv_bytes(m, n, d.F.nnz, sizeof(KT), sizeof(KT), sizeof(KT)) +
+                     (sub ? sizeof(KT) * (double)m : 0.0);
+          tm.sync();
+          for (int pass = 0; pass < o.reorth; ++pass)
+            cgs_pass(m, X, ldm, nX, wx);
+        } else {
+          const KT *xj = X + (int64_t)(nX - 1) * ldm;
+          const KT *yp = Y + (int64_t)(nY - 1) * ldn;
+          const KT bp = (KT)beta_prev;
+          if constexpr (sizeof(KT) == 8) {
+            team_spmv(tm, d.B.rows, d.B.rp, d.B.ci, d.B.v64, xj, d.B.lanes,
+                      [&](int64_t i, double s) { wy[i] = (KT)(s - (double)bp * (double)yp[i]); });
+          } else {
+            team_spmv(tm, d.B.rows, d.B.rp, d.B.ci, d.B.v32, xj, d.B.lanes,
+                      [&](int64_t i, float s) { wy[i] = (KT)(s - (float)bp * (float)yp[i]); });
+          }
+          count_B();
+          c.bytes += spmv_bytes(n, m, d.B.nnz, sizeof(KT), sizeof(KT), sizeof(KT)) + sizeof(KT) * (double)n;
+          tm.sync();
+          for (int pass = 0; pass < o.reorth; ++pass) {
+            cgs_pass(n, d.basis, d.ldb, (int)nb, wy);
+            cgs_pass(n, Y, ldn, nY, wy);
+          }
+        }
+        const int64_t len = from_y ? m : n;
+        KT *w = from_y ? wx : wy;
+        double bj;
+        if constexpr (sizeof(KT) == 8)
+          bj = nrm2(len, (const double *)w);
+        else {
+          bj = team_nrm2(tm, len, w);
+          c.bytes += 4.0 * len;
+        }
+        if (tm.leader())
+          d.alpha[na] = 0.0;
+        na++;
+        beta_last = bj;
+        if (!isfinite(bj) || bj < 1e-14 || nY + nX >= ncv)
+          break;
+        if (tm.leader())
+          d.beta[nbeta] = bj;
+        beta_prev = bj;
+        nbeta++;
+        KT *dst = from_y ? X + (int64_t)nX * ldm : Y + (int64_t)nY * ldn;
+        const double s = 1.0 / bj;
+        team_for(tm, len, [&](int64_t i) { dst[i] = (KT)((double)w[i] * s); });
+        c.bytes += 2.0 * sizeof(KT) * len;
+        tm.sync();
+        if (from_y)
+          nX++;
+        else
+          nY++;
+        ++local_steps;
+      }
+      c.steps += local_steps;
+      tm.publish(); // alpha/beta written by the leader
+      const int l = na;
+      if (l == 0 || !isfinite(beta_last) || !tm.ok())
+        break;
+
+      const bool split = (o.use_harmonic != 0) && o.target_tau == 0.0;
+      const int ncand = tiny_problem(l, beta_last, nY);
+      if (ncand < 0) {
+        random(y0);
+        gs2_basis(y0);
+        continue;
+      }
+
+      int64_t test_cap = k_target > 8 ? k_target : 8;
+      if (test_cap > l)
+        test_cap = l;
+      double best_res = INFINITY;
+      bool have_best = false, accepted_this = false, polish_stalled = false;
+      int64_t tested = 0;
+      const int ny_used = split ? ncand : (l + 1) / 2;
+      for (int t = 0; t < ncand && tested < test_cap && tm.ok(); ++t) {
+        const int jb = *(volatile int32_t *)&d.ord[t];
+        double ce2 = 0.0;
+        for (int q = 0; q < ny_used; q++) {
+          const double cq = coef(split, l, jb, q);
+          ce2 += cq * cq;
+        }
+        if (!(ce2 >= 1e-20))
+          continue;
+        // candidate v = sum_q coef_q Y[q]
+        if (threadIdx.x < (unsigned)ny_used)
+          tm.sh->h[threadIdx.x] = coef(split, l, jb, threadIdx.x);
+        __syncthreads();
+        team_for(tm, n, [&](int64_t i) {
+          double acc = 0.0;
+          for (int q = 0; q < ny_used; q++)
+            acc += tm.sh->h[q] * (double)Y[(int64_t)q * ldn + i];
+          v[i] = acc;
+        });
+        c.bytes += (double)(ny_used * sizeof(KT) + 8) * n;
+        tm.sync();
+        gs2_basis(v);
+        const double nv = nrm2(n, v);
+        if (!isfinite(nv) || nv < 1e-8)
+          continue;
+        scale(n, 1.0 / nv, v);
+        ++tested;
+        double res = mulF_norm(v, tmv);
+        if (!isfinite(res))
+          continue;
+        if (res > prescreen || polish_stalled) {
+          if (res < best_res) {
+            best_res = res;
+            copy(n, v, best_v);
+            have_best = true;
+          }
+          continue;
+        }
+        int64_t cg_its = 0;
+        bool hit_maxit = false;
+        const int passes = o.projector_passes > 1 ? o.projector_passes : 1;
+        for (int pass = 0; pass < passes && res > accept && tm.ok(); ++pass) {
+          double rn;
+          cg_its = cg(tmv, wm, o.cg_maxit, o.cg_rel_tol, o.cg_breakdown_tol, &rn);
+          c.cg_solves++;
+          if (cg_its >= o.cg_maxit) {
+            c.cg_maxit_hits++;
+            hit_maxit = true;
+          }
+          mulB(wm, tn);
+          team_for(tm, n, [&](int64_t i) { vp[i] = v[i] - tn[i]; });
+          c.bytes += 24.0 * n;
+          tm.sync();
+          gs2_basis(vp);
+          const double np = nrm2(n, vp);
+          if (!isfinite(np) || np < 1e-14)
+            break;
+          scale(n, 1.0 / np, vp);
+          const double res_p = mulF_norm(vp, wm);
+          if (!(res_p < res))
+            break;
+          double *t1 = v;
+          v = vp;
+          vp = t1;
+          res = res_p;
+          t1 = tmv;
+          tmv = wm;
+          wm = t1;
+        }
+        if (res <= accept) {
+          copy(n, v, d.basis + nb * d.ldb);
+          nb++;
+          accepted_this = true;
+          if (nb >= k_target) {
+            converged = true;
+            break;
+          }
+        } else {
+          polish_stalled = polish_stalled || hit_maxit;
+          if (res < best_res) {
+            best_res = res;
+            copy(n, v, best_v);
+            have_best = true;
+          }
+        }
+      }
+      if (converged)
+        break;
+      if (!accepted_this) {
+        ++rsa;
+        if (o.stagnation_restarts > 0 && rsa >= o.stagnation_restarts)
+          break;
+      } else {
+        rsa = 0;
+      }
+      if (have_best) {
+        copy(n, best_v, y0);
+      } else {
+        random(y0);
+        gs2_basis(y0);
+      }
+    }
+    if (!converged && nb < k_target && tm.ok()) {
+      int64_t failures = 0;
+      while (nb < k_target && failures < 8 && tm.ok()) {
+        if (try_project_random(accept))
+          failures = 0;
+        else
+          ++failures;
+      }
+      converged = nb >= k_target;
+    }
+    tm.sync();
+    if (tm.leader()) {
+      CyclicDevResult *R = d.res;
+      R->n_found = nb;
+      R->restarts = c.restarts;
+      R->krylov_steps_total = c.steps;
+      R->cg_solves = c.cg_solves;
+      R->cg_maxit_hits = c.cg_maxit_hits;
+      R->spmv = c.spmv;
+      R->spmvT = c.spmvT;
+      R->frob = frob;
+      R->bytes = c.bytes;
+      R->converged = converged ? 1 : 0;
+      R->status = *(volatile int *)d.status;
+    }
+  }
+};
+
+// Entry for the early exits of find_right_nullspace that need no work
+// (CyclicLanczosSolver.cpp:297-309) is handled on the host.
+
+template <class KT>
+__global__ void __launch_bounds__(512) cyclic_grid_kernel(CyclicDesc d) {
+  __shared__ TeamShared sh;
+  TeamGrid tm{&sh, d.status, d.gb, d.gpart, 0, 0};
+  CyclicSolver<TeamGrid, KT> s(tm, d);
+  s.run();
+}
+
+template <class KT>
+__global__ void __launch_bounds__(512) cyclic_cta_kernel(const CyclicDesc *descs, int count,
+                                                         int *queue) {
+  __shared__ TeamShared sh;
+  __shared__ int s_item;
+  for (;;) {
+    if (threadIdx.x == 0)
+      s_item = atomicAdd(queue, 1);
+    __syncthreads();
+    const int item = s_item;
+    __syncthreads();
+    if (item >= count)
+      break;
+    const CyclicDesc &d = descs[item];
+    TeamCta tm{&sh, d.status, 0};
+    CyclicSolver<TeamCta, KT> s(tm, d);
+    s.run();
+    __syncthreads();
+  }
+}
+
+} // namespace kr

@@ -1,0 +1,499 @@
+// Device building blocks of the KraNS B200 engine.
+//
+// The solvers are written once against a "team": the set of threads that
+// cooperates on one null-space solve.
+//   TeamCta  - one thread block (batched serving: many solves side by side,
+//              one per block, synchronised with __syncthreads).
+//   TeamGrid - every block of a cooperative launch (one large solve on the
+//              whole GPU, synchronised with a bounded grid barrier).
+// All reductions use a fixed tree whose shape depends only on the team size,
+// so a solve gives bit-identical results alone and inside a batch.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/krans_cuda.h"
+
+#define KR_DEV __device__ __forceinline__
+#define KR_MAX_WARPS 32
+#define KR_RED_K 8 // values per fused team reduction
+
+namespace kr {
+
+// ---------------------------------------------------------------------------
+// timing / barrier primitives
+// ---------------------------------------------------------------------------
+KR_DEV uint64_t globaltimer_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// A grid barrier wait gives up after this long and flags KRANS_ERR_TIMEOUT
+// (the longest legitimate wait is a serial section on the leader block).
+constexpr uint64_t kBarrierTimeoutNs = 8ull * 1000ull * 1000ull * 1000ull;
+
+struct GridBarrierState {
+  unsigned int count;
+  unsigned int gen;
+  int error; // sticky: once set, barriers return at once and solvers unwind
+  int pad;
+};
+
+// Per-block shared memory used by the team primitives.
+struct TeamShared {
+  double red[2][KR_MAX_WARPS * KR_RED_K]; // double-buffered warp partials
+  double bc[KR_RED_K];                    // broadcast slots (grid reductions)
+  double h[160];                          // Gram-Schmidt coefficients
+  int ibuf[64];                           // small integer scratch
+};
+
+KR_DEV double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1)
+    v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Block-level sum of K values; every thread receives the totals. Fixed order:
+// butterfly inside each warp, then warps summed in index order.
+template <int K>
+KR_DEV void block_sum(TeamShared *sh, int &buf, double (&v)[K]) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+  for (int k = 0; k < K; k++)
+    v[k] = warp_sum(v[k]);
+  double *r = sh->red[buf];
+  if (lane == 0) {
+#pragma unroll
+    for (int k = 0; k < K; k++)
+      r[wid * KR_RED_K + k] = v[k];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < K; k++) {
+    double s = 0.0;
+    for (int w = 0; w < nw; w++)
+      s += r[w * KR_RED_K + k];
+    v[k] = s;
+  }
+  buf ^= 1;
+}
+
+// ---------------------------------------------------------------------------
+// Teams
+// ---------------------------------------------------------------------------
+struct TeamCta {
+  TeamShared *sh;
+  int *err; // per-solve status word (global)
+  int buf;
+  KR_DEV int64_t tid() const { return threadIdx.x; }
+  KR_DEV int64_t nthreads() const { return blockDim.x; }
+  KR_DEV int64_t warp_id() const { return threadIdx.x >> 5; }
+  KR_DEV int64_t nwarps() const { return blockDim.x >> 5; }
+  KR_DEV bool lead_cta() const { return true; }
+  KR_DEV bool leader() const { return threadIdx.x == 0; }
+  KR_DEV bool ok() const { return *(volatile int *)err == 0; }
+  KR_DEV void sync() { __syncthreads(); }
+  template <int K> KR_DEV void sum(double (&v)[K]) { block_sum<K>(sh, buf, v); }
+  KR_DEV double sum1(double x) {
+    double v[1] = {x};
+    sum<1>(v);
+    return v[0];
+  }
+  // make values written by the leader block visible to the team
+  KR_DEV void publish() { __syncthreads(); }
+};
+
+struct TeamGrid {
+  TeamShared *sh;
+  int *err;
+  GridBarrierState *gb;
+  double *gpart; // [2][gridDim.x][KR_RED_K]
+  int buf;
+  int gbuf;
+  KR_DEV int64_t tid() const { return (int64_t)blockIdx.x * blockDim.x + threadIdx.x; }
+  KR_DEV int64_t nthreads() const { return (int64_t)gridDim.x * blockDim.x; }
+  KR_DEV int64_t warp_id() const { return tid() >> 5; }
+  KR_DEV int64_t nwarps() const { return nthreads() >> 5; }
+  KR_DEV bool lead_cta() const { return blockIdx.x == 0; }
+  KR_DEV bool leader() const { return blockIdx.x == 0 && threadIdx.x == 0; }
+  KR_DEV bool ok() const { return *(volatile int *)err == 0 && *(volatile int *)&gb->error == 0; }
+
+  // Sense-counting grid barrier with a bounded wait. On timeout it records
+  // KRANS_ERR_TIMEOUT in the solve's status word; afterwards every barrier
+  // returns immediately and the solver's bounded loops unwind.
+  KR_DEV void sync() {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      volatile int *verr = &gb->error;
+      if (*verr == 0) {
+        volatile unsigned *vgen = &gb->gen;
+        const unsigned g = *vgen;
+        __threadfence();
+        const unsigned arrived = atomicAdd(&gb->count, 1u);
+        if (arrived == gridDim.x - 1) {
+          atomicExch(&gb->count, 0u);
+          __threadfence();
+          atomicAdd(&gb->gen, 1u);
+        } else {
+          const uint64_t t0 = globaltimer_ns();
+          while (*vgen == g) {
+            if (*verr != 0)
+              break;
+            if (globaltimer_ns() - t0 > kBarrierTimeoutNs) {
+              atomicCAS(&gb->error, 0, KRANS_ERR_TIMEOUT);
+              atomicCAS(err, 0, KRANS_ERR_TIMEOUT);
+              break;
+            }
+            __nanosleep(40);
+          }
+        }
+        __threadfence();
+      }
+    }
+    __syncthreads();
+  }
+
+  template <int K> KR_DEV void sum(double (&v)[K]) {
+    block_sum<K>(sh, buf, v);
+    double *gp = gpart + (size_t)gbuf * gridDim.x * KR_RED_K;
+    if (threadIdx.x == 0) {
+#pragma unroll
+      for (int k = 0; k < K; k++)
+        gp[(size_t)blockIdx.x * KR_RED_K + k] = v[k];
+    }
+    sync();
+    // warp 0 of every block sums the block partials in the same fixed order
+    if (threadIdx.x < 32) {
+      const int lane = threadIdx.x;
+#pragma unroll
+      for (int k = 0; k < K; k++) {
+        double s = 0.0;
+        for (unsigned b = lane; b < gridDim.x; b += 32)
+          s += __ldcg(gp + (size_t)b * KR_RED_K + k);
+        s = warp_sum(s);
+        if (lane == 0)
+          sh->bc[k] = s;
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < K; k++)
+      v[k] = sh->bc[k];
+    __syncthreads();
+    gbuf ^= 1;
+  }
+  KR_DEV double sum1(double x) {
+    double v[1] = {x};
+    sum<1>(v);
+    return v[0];
+  }
+  KR_DEV void publish() { sync(); }
+};
+
+// ---------------------------------------------------------------------------
+// Element-wise team loops (grid-stride over the team's threads)
+// ---------------------------------------------------------------------------
+template <class Team, class F> KR_DEV void team_for(Team &tm, int64_t len, F f) {
+  const int64_t nt = tm.nthreads();
+  for (int64_t i = tm.tid(); i < len; i += nt)
+    f(i);
+}
+
+template <class T> KR_DEV double to_d(T x) { return (double)x; }
+
+template <class Team, class TX, class TY>
+KR_DEV double team_dot(Team &tm, int64_t len, const TX *x, const TY *y) {
+  double s = 0.0;
+  const int64_t nt = tm.nthreads();
+  for (int64_t i = tm.tid(); i < len; i += nt)
+    s += to_d(x[i]) * to_d(y[i]);
+  return tm.sum1(s);
+}
+
+template <class Team, class TX> KR_DEV double team_nrm2(Team &tm, int64_t len, const TX *x) {
+  double s = 0.0;
+  const int64_t nt = tm.nthreads();
+  for (int64_t i = tm.tid(); i < len; i += nt) {
+    const double v = to_d(x[i]);
+    s += v * v;
+  }
+  return sqrt(tm.sum1(s));
+}
+
+// h[q] = <S_q, w> for q < ns (S columns at stride ld); results in tm.sh->h
+// (all threads of every block see them after the call).
+template <class Team, class TS, class TW>
+KR_DEV void team_multidot(Team &tm, int64_t len, const TS *S, int64_t ld, int ns, const TW *w) {
+  const int64_t nt = tm.nthreads();
+  for (int q0 = 0; q0 < ns; q0 += KR_RED_K) {
+    double acc[KR_RED_K];
+#pragma unroll
+    for (int k = 0; k < KR_RED_K; k++)
+      acc[k] = 0.0;
+    const int qn = min(KR_RED_K, ns - q0);
+    for (int64_t i = tm.tid(); i < len; i += nt) {
+      const double wi = to_d(w[i]);
+#pragma unroll
+      for (int k = 0; k < KR_RED_K; k++)
+        if (k < qn)
+          acc[k] += to_d(S[(int64_t)(q0 + k) * ld + i]) * wi;
+    }
+    tm.template sum<KR_RED_K>(acc);
+    if (threadIdx.x < (unsigned)qn)
+      tm.sh->h[q0 + threadIdx.x] = acc[threadIdx.x];
+  }
+  __syncthreads();
+}
+
+// w -= sum_q S_q * coef[q]  (coef in shared memory), optional ||w||^2 out.
+template <class Team, class TS, class TW>
+KR_DEV void team_multi_axpy(Team &tm, int64_t len, const TS *S, int64_t ld, int ns,
+                            const double *coef, TW *w) {
+  const int64_t nt = tm.nthreads();
+  for (int64_t i = tm.tid(); i < len; i += nt) {
+    double acc = to_d(w[i]);
+    for (int q = 0; q < ns; q++)
+      acc -= to_d(S[(int64_t)q * ld + i]) * coef[q];
+    w[i] = (TW)acc;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// CSR SpMV inside a team: `lanes` threads per row (power of two <= 32), rows
+// handed out in warp-uniform blocks so the shuffles see full warps. The
+// epilogue gets (row, sum) on the first lane of the row group.
+// ---------------------------------------------------------------------------
+template <class Acc> struct AccOf;
+template <> struct AccOf<double> { using T = double; };
+template <> struct AccOf<float> { using T = float; };
+
+template <class Team, class VT, class XT, class Epi>
+KR_DEV void team_spmv(Team &tm, int64_t rows, const int32_t *__restrict__ rp,
+                      const int32_t *__restrict__ ci, const VT *__restrict__ val,
+                      const XT *__restrict__ x, int lanes, Epi epi) {
+  using Acc = typename AccOf<VT>::T;
+  const int lane = threadIdx.x & 31;
+  const int sub = lane & (lanes - 1);
+  const int rows_per_warp = 32 / lanes;
+  const int64_t nw = tm.nwarps();
+  for (int64_t base = tm.warp_id() * rows_per_warp; base < rows; base += nw * rows_per_warp) {
+    const int64_t i = base + lane / lanes;
+    Acc s = Acc(0);
+    if (i < rows) {
+      const int32_t b = __ldg(rp + i), e = __ldg(rp + i + 1);
+      for (int32_t k = b + sub; k < e; k += lanes)
+        s += (Acc)__ldg(val + k) * (Acc)x[__ldg(ci + k)];
+    }
+    for (int o = lanes >> 1; o > 0; o >>= 1)
+      s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (i < rows && sub == 0)
+      epi(i, s);
+  }
+}
+
+// Algorithmic HBM bytes of one CSR SpMV (rows r, cols c, nnz z, value width
+// w, x width wx, y width wy): row pointers, columns+values, x once, y once.
+__host__ __device__ inline double spmv_bytes(int64_t r, int64_t c, int64_t z, int w, int wx, int wy) {
+  return 4.0 * (double)(r + 1) + (double)z * (w + 4) + (double)c * wx + (double)r * wy;
+}
+
+// ---------------------------------------------------------------------------
+// Random normal vectors
+// ---------------------------------------------------------------------------
+// State of one factory stream. Layout of the MT part equals the CPU oracle's.
+struct RngState {
+  uint32_t mt[624];
+  int32_t idx;
+  int32_t has_saved;
+  double saved;
+  uint64_t philox_key;
+  uint64_t philox_ctr;
+  int32_t mode;
+  int32_t pad;
+};
+
+KR_DEV uint32_t mt_temper(uint32_t y) {
+  y ^= y >> 11;
+  y ^= (y << 7) & 0x9d2c5680u;
+  y ^= (y << 15) & 0xefc60000u;
+  y ^= y >> 18;
+  return y;
+}
+
+// Block-cooperative MT19937 regeneration of 624 words: src -> dst. The
+// recurrence new[i] = f(old[i], old[i+1], new-or-old[(i+397) mod 624]) is
+// evaluated in four dependency waves ([0,227), [227,454), [454,623), 623).
+KR_DEV void mt_regen_block(const uint32_t *src, uint32_t *dst) {
+  const int t = threadIdx.x;
+  auto f = [&](int i, uint32_t a, uint32_t b, uint32_t c) {
+    const uint32_t y = (a & 0x80000000u) | (b & 0x7fffffffu);
+    uint32_t v = c ^ (y >> 1);
+    if (y & 1u)
+      v ^= 0x9908b0dfu;
+    dst[i] = v;
+  };
+  for (int i = t; i < 227; i += blockDim.x)
+    f(i, src[i], src[i + 1], src[i + 397]);
+  __syncthreads();
+  for (int i = 227 + t; i < 454; i += blockDim.x)
+    f(i, src[i], src[i + 1], dst[i - 227]);
+  __syncthreads();
+  for (int i = 454 + t; i < 623; i += blockDim.x)
+    f(i, src[i], src[i + 1], dst[i - 227]);
+  __syncthreads();
+  if (t == 0)
+    f(623, src[623], dst[0], dst[396]);
+  __syncthreads();
+}
+
+// One block draws the next n normals of an MT19937 + polar stream, exactly
+// as std::normal_distribution<double> consumes std::mt19937 in libstdc++:
+// each polar attempt takes four 32-bit words (two 53-bit canonicals); an
+// accepted attempt yields y*m then x*m, and an unused x*m is carried over.
+// Needs blockDim.x >= 160.
+KR_DEV void block_mt_normals(RngState *st, double *out, int64_t n) {
+  __shared__ uint32_t smt[2][624];
+  __shared__ int s_wsum[8];
+  __shared__ int s_last;
+  __shared__ double s_saved;
+  __shared__ int s_has_saved;
+  int cur = 0;
+  for (int i = threadIdx.x; i < 624; i += blockDim.x)
+    smt[0][i] = st->mt[i];
+  int idx = st->idx;
+  if (threadIdx.x == 0) {
+    s_has_saved = st->has_saved;
+    s_saved = st->saved;
+  }
+  __syncthreads();
+  int64_t pos = 0;
+  if (n > 0 && s_has_saved) {
+    if (threadIdx.x == 0)
+      out[0] = s_saved;
+    pos = 1;
+    __syncthreads();
+    if (threadIdx.x == 0)
+      s_has_saved = 0;
+  }
+  __syncthreads();
+  const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
+  while (pos < n) {
+    if (idx >= 624) {
+      mt_regen_block(smt[cur], smt[cur ^ 1]);
+      cur ^= 1;
+      idx = 0;
+    }
+    const int navail = (624 - idx) >> 2;
+    bool acc = false;
+    double x = 0.0, y = 0.0, r2 = 0.0;
+    if (t < navail) {
+      const uint32_t *w = smt[cur] + idx + 4 * t;
+      const double a = (double)mt_temper(w[0]), b = (double)mt_temper(w[1]);
+      const double c = (double)mt_temper(w[2]), d = (double)mt_temper(w[3]);
+      double u1 = __dadd_rn(a, __dmul_rn(b, 4294967296.0)) * 0x1p-64;
+      double u2 = __dadd_rn(c, __dmul_rn(d, 4294967296.0)) * 0x1p-64;
+      if (u1 >= 1.0)
+        u1 = 0x1.fffffffffffffp-1;
+      if (u2 >= 1.0)
+        u2 = 0x1.fffffffffffffp-1;
+      x = __dadd_rn(__dmul_rn(2.0, u1), -1.0);
+      y = __dadd_rn(__dmul_rn(2.0, u2), -1.0);
+      r2 = __dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y));
+      acc = !(r2 > 1.0 || r2 == 0.0);
+    }
+    const unsigned bal = __ballot_sync(0xffffffffu, acc);
+    if (lane == 0 && wid < 8)
+      s_wsum[wid] = __popc(bal);
+    if (t == 0)
+      s_last = -1;
+    __syncthreads();
+    int before = __popc(bal & ((1u << lane) - 1u));
+    int total = 0;
+    for (int w = 0; w < 5; w++) {
+      if (w < wid)
+        before += s_wsum[w];
+      total += s_wsum[w];
+    }
+    const int64_t need = (n - pos + 1) >> 1; // pairs still needed
+    if (acc && before < need) {
+      const double mult = sqrt(-2.0 * log(r2) / r2);
+      const int64_t p = pos + 2 * (int64_t)before;
+      out[p] = __dmul_rn(y, mult);
+      if (p + 1 < n) {
+        out[p + 1] = __dmul_rn(x, mult);
+      } else {
+        s_saved = __dmul_rn(x, mult);
+        s_has_saved = 1;
+      }
+      if (before == need - 1)
+        s_last = t;
+    }
+    __syncthreads();
+    if (total >= need) {
+      idx += 4 * (s_last + 1);
+      pos = n;
+    } else {
+      idx += 4 * navail;
+      pos += 2 * (int64_t)total;
+    }
+    __syncthreads();
+  }
+  for (int i = threadIdx.x; i < 624; i += blockDim.x)
+    st->mt[i] = smt[cur][i];
+  if (threadIdx.x == 0) {
+    st->idx = idx;
+    st->has_saved = s_has_saved;
+    st->saved = s_saved;
+  }
+  __syncthreads();
+}
+
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw: "Parallel random numbers: as
+// easy as 1, 2, 3", SC'11), counter-based.
+KR_DEV uint4 philox4x32_10(uint4 c, uint2 k) {
+#pragma unroll
+  for (int r = 0; r < 10; r++) {
+    const uint32_t hi0 = __umulhi(0xD2511F53u, c.x), lo0 = 0xD2511F53u * c.x;
+    const uint32_t hi1 = __umulhi(0xCD9E8D57u, c.z), lo1 = 0xCD9E8D57u * c.z;
+    c = make_uint4(hi1 ^ c.y ^ k.x, lo1, hi0 ^ c.w ^ k.y, lo0);
+    k.x += 0x9E3779B9u;
+    k.y += 0xBB67AE85u;
+  }
+  return c;
+}
+
+// Normal variate number `ctr` of the stream `key` (Box-Muller on two
+// 53-bit uniforms from one Philox block).
+KR_DEV double philox_normal(uint64_t key, uint64_t ctr) {
+  const uint4 r = philox4x32_10(make_uint4((uint32_t)ctr, (uint32_t)(ctr >> 32), 0x4b52414eu, 0u),
+                                make_uint2((uint32_t)key, (uint32_t)(key >> 32)));
+  const uint64_t a = ((uint64_t)r.x << 21) ^ (uint64_t)(r.y >> 11);
+  const uint64_t b = ((uint64_t)r.z << 21) ^ (uint64_t)(r.w >> 11);
+  const double u1 = ((double)(a & ((1ull << 53) - 1)) + 1.0) * 0x1p-53; // (0, 1]
+  const double u2 = (double)(b & ((1ull << 53) - 1)) * 0x1p-53;         // [0, 1)
+  return sqrt(-2.0 * log(u1)) * cospi(2.0 * u2);
+}
+
+// Fill out[0..n) with the stream's next n normals, as a team. MT19937 is
+// generated by the team's leader block; Philox by every thread.
+template <class Team> KR_DEV void team_random_normal(Team &tm, RngState *st, double *out, int64_t n) {
+  if (*(volatile int32_t *)&st->mode == KRANS_RNG_PHILOX) {
+    const uint64_t key = *(volatile uint64_t *)&st->philox_key;
+    const uint64_t base = *(volatile uint64_t *)&st->philox_ctr;
+    team_for(tm, n, [&](int64_t i) { out[i] = philox_normal(key, base + (uint64_t)i); });
+    tm.sync();
+    if (tm.leader())
+      st->philox_ctr = base + (uint64_t)n;
+    tm.publish();
+  } else {
+    if (tm.lead_cta())
+      block_mt_normals(st, out, n);
+    tm.publish();
+  }
+}
+
+} // namespace kr

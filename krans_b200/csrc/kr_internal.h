@@ -1,0 +1,82 @@
+// Host-side internal declarations shared by the library's translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdint>
+#include <cstdio>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/krans_cuda.h"
+
+namespace kr {
+
+void set_error(const char *fmt, ...);
+int cuda_fail(cudaError_t e, const char *what, const char *file, int line);
+
+#define KR_CUDA(call)                                                                       \
+  do {                                                                                      \
+    cudaError_t e_ = (call);                                                                \
+    if (e_ != cudaSuccess)                                                                  \
+      return ::kr::cuda_fail(e_, #call, __FILE__, __LINE__);                               \
+  } while (0)
+
+#define KR_CHECK_ARG(cond, msg)                                                             \
+  do {                                                                                      \
+    if (!(cond)) {                                                                          \
+      ::kr::set_error("%s", msg);                                                           \
+      return KRANS_ERR_INVALID_ARGUMENT;                                                    \
+    }                                                                                       \
+  } while (0)
+
+struct RngState;
+struct GridBarrierState;
+
+} // namespace kr
+
+struct krans_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  size_t budget = 0;
+  size_t in_use = 0;
+  int sms = 0;
+  int cc_major = 0, cc_minor = 0;
+  double *h_scalar = nullptr; // pinned scalars for D2H reads
+  double *d_scalar = nullptr; // device scalars (reductions)
+  double *d_partials = nullptr;
+  int partial_blocks = 0;
+  std::mutex mu;
+};
+
+struct krans_mat {
+  krans_ctx *ctx = nullptr;
+  int64_t m = 0, n = 0, nnz = 0;
+  int32_t *rp = nullptr, *ci = nullptr, *rpT = nullptr, *ciT = nullptr;
+  double *v = nullptr, *vT = nullptr;
+  float *v32 = nullptr, *vT32 = nullptr;
+  int lanes = 1, lanesT = 1;
+  size_t bytes = 0;
+};
+
+struct krans_vec {
+  krans_ctx *ctx = nullptr;
+  int64_t n = 0;
+  double *d = nullptr;
+};
+
+struct krans_rng {
+  krans_ctx *ctx = nullptr;
+  kr::RngState *d = nullptr;
+  uint32_t seed = 0;
+  int mode = 0;
+};
+
+namespace kr {
+// allocation with budget accounting
+int dev_alloc(krans_ctx *ctx, void **p, size_t bytes);
+void dev_free(krans_ctx *ctx, void *p, size_t bytes);
+int pick_lanes(int64_t rows, int64_t nnz);
+} // namespace kr
