@@ -95,6 +95,8 @@ struct TeamCta {
   KR_DEV int64_t nwarps() const { return blockDim.x >> 5; }
   KR_DEV bool lead_cta() const { return true; }
   KR_DEV bool leader() const { return threadIdx.x == 0; }
+  KR_DEV int cta_rank() const { return 0; }
+  KR_DEV int ncta() const { return 1; }
   KR_DEV bool ok() const { return *(volatile int *)err == 0; }
   KR_DEV void sync() { __syncthreads(); }
   template <int K> KR_DEV void sum(double (&v)[K]) { block_sum<K>(sh, buf, v); }
@@ -120,6 +122,8 @@ struct TeamGrid {
   KR_DEV int64_t nwarps() const { return nthreads() >> 5; }
   KR_DEV bool lead_cta() const { return blockIdx.x == 0; }
   KR_DEV bool leader() const { return blockIdx.x == 0 && threadIdx.x == 0; }
+  KR_DEV int cta_rank() const { return blockIdx.x; }
+  KR_DEV int ncta() const { return gridDim.x; }
   KR_DEV bool ok() const { return *(volatile int *)err == 0 && *(volatile int *)&gb->error == 0; }
 
   // Sense-counting grid barrier with a bounded wait. On timeout it records
@@ -204,6 +208,7 @@ template <class Team, class F> KR_DEV void team_for(Team &tm, int64_t len, F f) 
 }
 
 template <class T> KR_DEV double to_d(T x) { return (double)x; }
+KR_DEV int64_t imin64(int64_t a, int64_t b) { return a < b ? a : b; }
 
 template <class Team, class TX, class TY>
 KR_DEV double team_dot(Team &tm, int64_t len, const TX *x, const TY *y) {

@@ -1,0 +1,732 @@
+// Block LOBPCG on N = A^T A for the right null space, on the device.
+//
+// Restates find_nullspace_lobpcg_ex of the reference
+// (src/Solvers/LOBPCGSolver.cpp:443-834) as team code, including
+// orthonormalize_block (137-160), the tiny generalized eigenproblem with
+// Cholesky jitter (88-119), block_rr_polish (286-440) and
+// two_vec_rr_sharpen (199-278). Blocks are column-major (one contiguous
+// n-vector per column, leading dimension ldn). Dot products of a column
+// against a group of columns are fused into team reductions; Gram
+// matrices are formed in FP64 (tensor cores: kr_gram.cuh). Only
+// rounding differs from the reference: classical GS passes replace MGS
+// loops, and reductions use fixed trees.
+#pragma once
+
+#include "kr_cyclic.cuh"
+#include "kr_dense.cuh"
+#include "kr_device.cuh"
+#include "kr_gram.cuh"
+
+namespace kr {
+
+struct LobpcgDevResult {
+  int64_t n_right, iters, locked, block_size;
+  double frob, accept, best_unaccepted;
+  int32_t converged, status;
+  int32_t err_code, pad;
+  int64_t spmv, spmvT;
+  double bytes, gram_flops;
+};
+
+// error codes of the reference's throws (reported as KRANS_ERR_RUNTIME)
+enum LobpcgErr {
+  kLobErrNone = 0,
+  kLobErrInitialDependent = 1, // "LOBPCG: initial block is dependent"
+  kLobErrRestartOrth = 2,      // "LOBPCG: restart orthogonalization failed"
+  kLobErrXSlice = 3,           // "LOBPCG: X slice orthonormalization failed"
+  kLobErrGep = 4,              // "LOBPCG tiny GEP: S not SPD (after jitter)"
+  kLobErrTinyDim = 5,          // "LOBPCG: tiny problem too large (nv cap)"
+};
+
+struct LobpcgDesc {
+  CsrView F, B; // A (m x n) and A^T
+  krans_lobpcg_opts o;
+  int64_t k_target, bs, guards;
+  RngState *rng;
+  double *const *initial; // n_initial device vectors (or nullptr)
+  int64_t n_initial;
+  // blocks (column-major, ld = ldn)
+  double *X, *AX, *Rb, *W, *P, *T1, *T2, *Z, *AZ;
+  double *Yl, *RN; // locked set and output basis (k_target columns)
+  double *tmv, *vacc;
+  double *theta, *th;
+  // small dense matrices (pmax x pmax)
+  double *S, *G, *Ym, *Sj, *Li, *Tm, *Cm, *Q;
+  double *eig_cs;
+  int32_t *eig_pq, *eig_ord;
+  double *gram_part;
+  double *theta_out, *resid_out; // k_target
+  // polish scratch
+  double *pr, *pg, *ptmp;              // m, n, m
+  double *Vb, *D, *Vn, *Zp, *AZp;      // k, k+2, k, 2k+2, 2k+2 columns
+  double *sv_av, *sv_t, *sv_d, *sv_ad, *sv_nd, *sv_vn; // sharpen scratch
+  int64_t ldn, ldm, pmax;
+  int32_t *status;
+  LobpcgDevResult *res;
+  GridBarrierState *gb;
+  double *gpart;
+  int32_t *flag; // uniform scalar broadcast slot (leader writes, all read)
+  double *dflag;
+};
+
+template <class Team> struct LobpcgSolver {
+  Team &tm;
+  const LobpcgDesc &d;
+  int64_t m, n, ldn;
+  Counters c;
+  double gram_flops = 0.0;
+  int err = 0;
+
+  KR_DEV LobpcgSolver(Team &t, const LobpcgDesc &dd) : tm(t), d(dd) {
+    m = d.F.rows;
+    n = d.F.cols;
+    ldn = d.ldn;
+  }
+  KR_DEV double *col(double *b, int64_t j) const { return b + j * ldn; }
+
+  // ---- primitives ---------------------------------------------------------
+  KR_DEV void mulA(const double *x, double *y) {
+    team_spmv(tm, d.F.rows, d.F.rp, d.F.ci, d.F.v64, x, d.F.lanes, [&](int64_t i, double s) { y[i] = s; });
+    c.spmv++;
+    c.bytes += spmv_bytes(m, n, d.F.nnz, 8, 8, 8);
+    tm.sync();
+  }
+  KR_DEV void mulAT(const double *x, double *y) {
+    team_spmv(tm, d.B.rows, d.B.rp, d.B.ci, d.B.v64, x, d.B.lanes, [&](int64_t i, double s) { y[i] = s; });
+    c.spmvT++;
+    c.bytes += spmv_bytes(n, m, d.B.nnz, 8, 8, 8);
+    tm.sync();
+  }
+  KR_DEV double normA(const double *x, double *y) { // ||A x||, y = A x
+    double s2 = 0.0;
+    team_spmv(tm, d.F.rows, d.F.rp, d.F.ci, d.F.v64, x, d.F.lanes, [&](int64_t i, double s) {
+      y[i] = s;
+      s2 += s * s;
+    });
+    c.spmv++;
+    c.bytes += spmv_bytes(m, n, d.F.nnz, 8, 8, 8);
+    return sqrt(tm.sum1(s2));
+  }
+  KR_DEV double dot(const double *a, const double *b) {
+    c.bytes += 16.0 * n;
+    return team_dot(tm, n, a, b);
+  }
+  KR_DEV double nrm(const double *a) {
+    c.bytes += 8.0 * n;
+    return team_nrm2(tm, n, a);
+  }
+  KR_DEV void copy(const double *s, double *dd) {
+    team_for(tm, n, [&](int64_t i) { dd[i] = s[i]; });
+    c.bytes += 16.0 * n;
+    tm.sync();
+  }
+  KR_DEV void scale(double a, double *x) {
+    team_for(tm, n, [&](int64_t i) { x[i] *= a; });
+    c.bytes += 16.0 * n;
+    tm.sync();
+  }
+  KR_DEV void axpy(double a, const double *x, double *y) {
+    team_for(tm, n, [&](int64_t i) { y[i] += a * x[i]; });
+    c.bytes += 24.0 * n;
+    tm.sync();
+  }
+  KR_DEV void random(double *out) {
+    team_random_normal(tm, d.rng, out, n);
+    c.bytes += 8.0 * n;
+  }
+  // x -= sum_q <x, B_q> B_q over nb columns (one classical pass); when
+  // skip_zero, coefficients that are exactly 0 are dropped (project_out).
+  KR_DEV void gs_pass(const double *Bk, int64_t nb, double *x) {
+    if (nb <= 0)
+      return;
+    for (int64_t q0 = 0; q0 < nb; q0 += 128) {
+      const int cnt = (int)imin64(128, nb - q0);
+      team_multidot(tm, n, Bk + q0 * ldn, ldn, cnt, x);
+      team_multi_axpy(tm, n, Bk + q0 * ldn, ldn, cnt, tm.sh->h, x);
+      c.bytes += (double)(2 * cnt + 3) * 8.0 * n;
+      tm.sync();
+    }
+  }
+  // same against an arbitrary list of columns given by index set of a block
+  KR_DEV void gs_pass_excl(const double *Bk, int64_t nb, int64_t excl, double *x) {
+    // project x against columns q != excl, one at a time in the group form
+    for (int64_t q0 = 0; q0 < nb; q0 += 128) {
+      const int cnt = (int)imin64(128, nb - q0);
+      team_multidot(tm, n, Bk + q0 * ldn, ldn, cnt, x);
+      if (excl >= q0 && excl < q0 + cnt && threadIdx.x == 0)
+        tm.sh->h[excl - q0] = 0.0;
+      __syncthreads();
+      team_multi_axpy(tm, n, Bk + q0 * ldn, ldn, cnt, tm.sh->h, x);
+      c.bytes += (double)(2 * cnt + 3) * 8.0 * n;
+      tm.sync();
+    }
+  }
+
+  // MGS with optional reorth (GramSchmidt.cpp:55-82) on k columns of block V.
+  KR_DEV bool mgs(double *V, int64_t k, double tol, bool reorth) {
+    for (int64_t i = 0; i < k; i++) {
+      double *vi = col(V, i);
+      gs_pass(V, i, vi);
+      double n1 = nrm(vi);
+      if (n1 < tol)
+        return false;
+      if (reorth) {
+        gs_pass(V, i, vi);
+        const double n2 = nrm(vi);
+        if (n2 < tol)
+          return false;
+        n1 = n2;
+      }
+      scale(1.0 / n1, vi);
+    }
+    return true;
+  }
+
+  // orthonormalize_block (LOBPCGSolver.cpp:137-160): project each column vs
+  // basis and normalise (in place), then MGS on a copy in `scratch`, copied
+  // back only on success.
+  KR_DEV bool orthonormalize_block(double *Xb, int64_t k, const double *basis, int64_t nb, double tol,
+                                   bool reorth, double *scratch) {
+    for (int64_t i = 0; i < k; i++) {
+      double *xi = col(Xb, i);
+      gs_pass(basis, nb, xi);
+      const double nr = nrm(xi);
+      if (nr < tol)
+        return false;
+      scale(1.0 / nr, xi);
+    }
+    for (int64_t i = 0; i < k; i++)
+      copy(col(Xb, i), col(scratch, i));
+    if (!mgs(scratch, k, tol, reorth))
+      return false;
+    for (int64_t i = 0; i < k; i++)
+      copy(col(scratch, i), col(Xb, i));
+    return true;
+  }
+
+  KR_DEV void apply_normal(const double *Zb, int64_t k, double *AZb) {
+    for (int64_t j = 0; j < k; j++) {
+      mulA(col((double *)Zb, j), d.tmv);
+      mulAT(d.tmv, col(AZb, j));
+    }
+  }
+
+  KR_DEV void form_gram(const double *Zb, const double *AZb, int p) {
+    team_gram2(tm, n, Zb, AZb, ldn, p, d.S, d.G, d.gram_part);
+    gram_flops += 2.0 * 2.0 * (double)n * p * p;
+    c.bytes += 2.0 * 8.0 * n * p;
+  }
+
+  // solve_tiny_gep (LOBPCGSolver.cpp:88-119) on the leader block; theta in
+  // d.th, eigenvectors in d.Ym (ld p). Returns false if S is not SPD.
+  KR_DEV bool tiny_gep(int p) {
+    if (tm.lead_cta())
+      gep_block(p);
+    tm.publish();
+    return *(volatile int32_t *)d.flag == 0;
+  }
+  KR_DEV void gep_block(int p) {
+    double *S = d.S, *G = d.G;
+    // symmetrize
+    for (int e = threadIdx.x; e < p * p; e += blockDim.x) {
+      const int j = e / p, i = e % p;
+      if (i >= j) {
+        const double g = 0.5 * (G[i + (size_t)j * p] + G[j + (size_t)i * p]);
+        const double s = 0.5 * (S[i + (size_t)j * p] + S[j + (size_t)i * p]);
+        G[i + (size_t)j * p] = g;
+        G[j + (size_t)i * p] = g;
+        S[i + (size_t)j * p] = s;
+        S[j + (size_t)i * p] = s;
+      }
+    }
+    __syncthreads();
+    __shared__ double s_norm;
+    {
+      double s = 0.0;
+      for (int e = threadIdx.x; e < p * p; e += blockDim.x)
+        s += S[e] * S[e];
+      int b = 0;
+      double v[1] = {s};
+      block_sum<1>(tm.sh, b, v);
+      if (threadIdx.x == 0)
+        s_norm = fmax(1.0, sqrt(v[0]));
+      __syncthreads();
+    }
+    const double jit[4] = {0.0, 1e-14, 1e-12, 1e-10};
+    int ok = 0;
+    for (int t = 0; t < 4 && !ok; t++) {
+      for (int e = threadIdx.x; e < p * p; e += blockDim.x) {
+        double v = S[e];
+        if (jit[t] > 0.0 && (e % p) == (e / p))
+          v += jit[t] * s_norm;
+        d.Sj[e] = v;
+      }
+      __syncthreads();
+      if (block_cholesky(p, d.Sj) != 0)
+        continue;
+      block_lower_inverse(p, d.Sj, d.Li);
+      block_gemm_nn(p, d.Li, false, G, false, d.Tm);  // T = Li G
+      block_gemm_nn(p, d.Tm, false, d.Li, true, d.Cm); // C = T Li^T
+      block_jacobi_eig(p, d.Cm, d.th, d.Q, d.eig_cs, d.eig_pq, d.eig_ord);
+      __shared__ int s_fin;
+      if (threadIdx.x == 0)
+        s_fin = 1;
+      __syncthreads();
+      for (int i = threadIdx.x; i < p; i += blockDim.x)
+        if (!isfinite(d.th[i]))
+          s_fin = 0;
+      __syncthreads();
+      if (!s_fin)
+        continue;
+      block_gemm_nn(p, d.Li, true, d.Q, false, d.Ym); // Y = Li^T Q
+      ok = 1;
+    }
+    if (threadIdx.x == 0)
+      *d.flag = ok ? 0 : 1;
+    __syncthreads();
+  }
+
+  // out[i] = sum_{j<zc} Y(roff+j, i) Z_j for i < q (Y has leading dim ldy)
+  KR_DEV void combine(const double *Zb, int zc, const double *Y, int ldy, int roff, int q, double *out) {
+    team_combine(tm, n, Zb, ldn, zc, Y, ldy, roff, q, out);
+    c.bytes += (double)(zc + q) * 8.0 * n;
+    tm.sync();
+  }
+
+  KR_DEV void theta_from(int64_t bs, int tn) {
+    if (tm.leader()) {
+      for (int64_t j = 0; j < bs; j++)
+        d.theta[j] = 0.0;
+      const int64_t lim = tn < bs ? tn : bs;
+      for (int64_t j = 0; j < lim; j++)
+        d.theta[j] = fmax(0.0, d.th[j]);
+    }
+    tm.publish();
+  }
+  KR_DEV double theta_of(int64_t j) const { return *(volatile double *)&d.theta[j]; }
+
+  // ---- two_vec_rr_sharpen (LOBPCGSolver.cpp:199-278) ------------------------
+  KR_DEV bool sharpen(double *V, int64_t k, int64_t idx, double target, int max_iters) {
+    if (idx >= k)
+      return true;
+    double *Av = d.sv_av, *t = d.sv_t, *dd = d.sv_d, *Ad = d.sv_ad, *Nd = d.sv_nd, *vn = d.sv_vn;
+    double *vi = col(V, idx);
+    for (int it = 0; it < max_iters && tm.ok(); ++it) {
+      const double res = normA(vi, Av);
+      if (res <= target)
+        return true;
+      mulAT(Av, t);
+      copy(t, dd);
+      gs_pass_excl(V, k, idx, dd);
+      const double nd = nrm(dd);
+      if (nd <= 1e-14)
+        return false;
+      scale(1.0 / fmax(nd, 1e-300), dd);
+      mulA(dd, Ad);
+      mulAT(Ad, Nd);
+      double acc[4] = {0, 0, 0, 0};
+      team_for(tm, n, [&](int64_t i) {
+        acc[0] += vi[i] * t[i];
+        acc[1] += vi[i] * Nd[i];
+        acc[2] += dd[i] * t[i];
+        acc[3] += dd[i] * Nd[i];
+      });
+      tm.template sum<4>(acc);
+      c.bytes += 32.0 * n;
+      const double a = acc[0], g = 0.5 * (acc[2] + acc[1]), e = acc[3];
+      double y0, y1;
+      if (g == 0.0) {
+        if (a <= e) {
+          y0 = 1.0;
+          y1 = 0.0;
+        } else {
+          y0 = 0.0;
+          y1 = 1.0;
+        }
+      } else {
+        const double theta = (e - a) / (2.0 * g);
+        const double tt = copysign(1.0, theta) / (fabs(theta) + sqrt(theta * theta + 1.0));
+        const double cc = 1.0 / sqrt(tt * tt + 1.0), s = tt * cc;
+        if (a - tt * g <= e + tt * g) {
+          y0 = cc;
+          y1 = -s;
+        } else {
+          y0 = s;
+          y1 = cc;
+        }
+      }
+      if (!isfinite(y0) || !isfinite(y1))
+        return false;
+      team_for(tm, n, [&](int64_t i) { vn[i] = vi[i] * y0 + y1 * dd[i]; });
+      tm.sync();
+      gs_pass_excl(V, k, idx, vn);
+      const double nv = nrm(vn);
+      if (nv <= 1e-14)
+        return false;
+      scale(1.0 / nv, vn);
+      copy(vn, vi);
+    }
+    return false;
+  }
+
+  // ---- block_rr_polish (LOBPCGSolver.cpp:286-440) ---------------------------
+  KR_DEV bool polish(double *V, int64_t k, double target, int max_sweeps) {
+    if (k == 0)
+      return true;
+    double *r = d.pr, *g = d.pg, *tmp = d.ptmp;
+    mgs(V, k, 1e-14, true);
+    for (int sweep = 0; sweep < max_sweeps && tm.ok(); ++sweep) {
+      double max_res = 0.0;
+      for (int64_t i = 0; i < k; i++)
+        max_res = fmax(max_res, normA(col(V, i), r));
+      if (max_res <= target)
+        break;
+      int64_t nd = 0;
+      for (int64_t i = 0; i < k; i++)
+        copy(col(V, i), col(d.Vb, i));
+      for (int64_t j = 0; j < k; j++) {
+        const double res = normA(col(V, j), r);
+        if (res <= target)
+          continue;
+        mulAT(r, g);
+        gs_pass(d.Vb, k, g);
+        const double gn = nrm(g);
+        if (gn <= 1e-14)
+          continue;
+        scale(1.0 / gn, g);
+        bool dup = false;
+        if (nd > 0) {
+          team_multidot(tm, n, d.D, ldn, (int)nd, g);
+          for (int64_t q = 0; q < nd; q++)
+            if (fabs(tm.sh->h[q]) >= 1.0 - 1e-8)
+              dup = true;
+          __syncthreads();
+        }
+        if (!dup) {
+          copy(g, col(d.D, nd));
+          nd++;
+        }
+      }
+      if (nd == 0) {
+        for (int64_t i = 0; i < k; i++) {
+          double *vi = col(V, i);
+          for (int it = 0; it < 50 && tm.ok(); ++it) {
+            const double res = normA(vi, r);
+            if (res <= target)
+              break;
+            mulAT(r, g);
+            gs_pass_excl(V, k, i, g);
+            const double gg = dot(g, g);
+            if (gg <= 0.0)
+              break;
+            const double ag = normA(g, tmp);
+            const double Ag2 = ag * ag;
+            if (Ag2 <= 0.0)
+              break;
+            axpy(-(gg / Ag2), g, vi);
+            gs_pass_excl(V, k, i, vi);
+            const double nv = nrm(vi);
+            if (nv > 0.0)
+              scale(1.0 / nv, vi);
+          }
+        }
+        mgs(V, k, 1e-14, true);
+        const int enrich = k < 2 ? (int)k : 2;
+        for (int e = 0; e < enrich; e++) {
+          double *q = col(d.D, nd);
+          random(q);
+          gs_pass(d.Vb, k, q);
+          const double nq = nrm(q);
+          if (nq > 1e-14) {
+            scale(1.0 / nq, q);
+            nd++;
+          }
+        }
+        if (nd > 0)
+          (void)orthonormalize_block(d.D, nd, d.Vb, k, 1e-14, true, d.Vn);
+        else
+          continue;
+      }
+      if (!orthonormalize_block(d.D, nd, d.Vb, k, 1e-14, true, d.Vn))
+        continue;
+      const int64_t zc = k + nd;
+      for (int64_t i = 0; i < k; i++)
+        copy(col(V, i), col(d.Zp, i));
+      for (int64_t i = 0; i < nd; i++)
+        copy(col(d.D, i), col(d.Zp, k + i));
+      apply_normal(d.Zp, zc, d.AZp);
+      form_gram(d.Zp, d.AZp, (int)zc);
+      if (!tiny_gep((int)zc)) {
+        err = kLobErrGep;
+        return false;
+      }
+      combine(d.Zp, (int)zc, d.Ym, (int)zc, 0, (int)k, d.Vn);
+      mgs(d.Vn, k, 1e-14, true);
+      for (int64_t i = 0; i < k; i++)
+        copy(col(d.Vn, i), col(V, i));
+      max_res = 0.0;
+      for (int64_t i = 0; i < k; i++)
+        max_res = fmax(max_res, normA(col(V, i), r));
+      if (max_res <= target)
+        break;
+    }
+    mgs(V, k, 1e-14, true);
+    return true;
+  }
+
+  KR_DEV void run() {
+    const krans_lobpcg_opts &o = d.o;
+    const int64_t bs = d.bs, k_target = d.k_target, guards = d.guards;
+    LobpcgDevResult R;
+    memset(&R, 0, sizeof R);
+    R.block_size = bs;
+    double *X = d.X, *AX = d.AX, *Rb = d.Rb, *W = d.W, *P = d.P, *T1 = d.T1, *T2 = d.T2;
+    int64_t nlocked = 0, nright = 0, its = 0;
+
+    // ||A||_F estimate (LOBPCGSolver.cpp:163-178)
+    {
+      const int samples = o.frob_samples > 1 ? o.frob_samples : 1;
+      double sum2 = 0.0;
+      for (int s = 0; s < samples; s++) {
+        random(d.vacc);
+        const double nr = normA(d.vacc, d.tmv);
+        sum2 += nr * nr;
+      }
+      R.frob = sqrt(sum2 / (double)samples);
+    }
+    const double accept_thr = fmax(o.tol_abs, o.tol_rel * fmax(1.0, R.frob));
+    R.accept = accept_thr;
+
+    // initial block: seeds, then random
+    int64_t filled = 0;
+    const int64_t seeds = d.initial ? min(d.n_initial, bs) : 0;
+    for (; filled < seeds; ++filled)
+      copy(d.initial[filled], col(X, filled));
+    for (; filled < bs; ++filled)
+      random(col(X, filled));
+    if (!orthonormalize_block(X, bs, d.Yl, 0, o.gs_tol, o.gs_reorth != 0, T1)) {
+      err = kLobErrInitialDependent;
+      goto finish;
+    }
+    apply_normal(X, bs, AX);
+    form_gram(X, AX, (int)bs);
+    if (!tiny_gep((int)bs)) {
+      err = kLobErrGep;
+      goto finish;
+    }
+    combine(X, (int)bs, d.Ym, (int)bs, 0, (int)bs, T1);
+    for (int64_t j = 0; j < bs; j++)
+      copy(col(T1, j), col(X, j));
+    apply_normal(X, bs, AX);
+    theta_from(bs, (int)bs);
+
+    while (nlocked < k_target && its < o.max_iters && tm.ok()) {
+      ++its;
+      int64_t nconv = 0;
+      double best_unacc = INFINITY;
+      for (int64_t j = 0; j < bs; ++j) {
+        const double th = theta_of(j);
+        double *rj = col(Rb, j), *xj = col(X, j), *axj = col(AX, j);
+        team_for(tm, n, [&](int64_t i) { rj[i] = axj[i] - th * xj[i]; });
+        c.bytes += 24.0 * n;
+        tm.sync();
+        const double av_orig = normA(xj, d.tmv);
+        if (av_orig <= accept_thr) {
+          copy(xj, d.vacc);
+          gs_pass(d.Yl, nlocked, d.vacc);
+          const double nv = nrm(d.vacc);
+          bool reject = false;
+          if (nv <= fmax(1e-14, 10.0 * o.gs_tol)) {
+            reject = true;
+          } else {
+            scale(1.0 / nv, d.vacc);
+            if (nlocked > 0) {
+              for (int64_t q0 = 0; q0 < nlocked; q0 += 128) {
+                const int cnt = (int)imin64(128, nlocked - q0);
+                team_multidot(tm, n, d.Yl + q0 * ldn, ldn, cnt, d.vacc);
+                for (int q = 0; q < cnt; q++)
+                  if (fabs(tm.sh->h[q]) >= 1.0 - 1e-8)
+                    reject = true;
+                __syncthreads();
+              }
+            }
+          }
+          double av_acc = INFINITY;
+          if (!reject) {
+            av_acc = normA(d.vacc, d.tmv);
+            if (av_acc > accept_thr)
+              reject = true;
+          }
+          if (!reject) {
+            copy(d.vacc, col(d.Yl, nlocked));
+            copy(d.vacc, col(d.RN, nright));
+            if (tm.leader()) {
+              d.theta_out[nright] = th;
+              d.resid_out[nright] = av_acc;
+            }
+            nright++;
+            nlocked++;
+            nconv++;
+            if (nlocked >= k_target)
+              break;
+          } else {
+            best_unacc = fmin(best_unacc, av_orig);
+          }
+        } else {
+          best_unacc = fmin(best_unacc, av_orig);
+        }
+      }
+      R.locked = nlocked;
+      R.iters = its;
+      R.best_unaccepted = isfinite(best_unacc) ? best_unacc : 0.0;
+      if (nlocked >= k_target)
+        break;
+
+      const int64_t ini = o.soft_locking ? nconv : 0;
+      if (nconv >= bs - guards) {
+        const int64_t remain = bs - nconv;
+        for (int64_t j = 0; j < remain; j++) {
+          copy(col(X, nconv + j), col(X, j));
+          copy(col(AX, nconv + j), col(AX, j));
+          copy(col(P, nconv + j), col(P, j));
+        }
+        if (tm.leader())
+          for (int64_t j = 0; j < remain; j++)
+            d.theta[j] = d.theta[nconv + j];
+        tm.publish();
+        for (int64_t j = remain; j < bs; j++)
+          random(col(X, j));
+        if (!orthonormalize_block(X, bs, d.Yl, nlocked, o.gs_tol, o.gs_reorth != 0, T1)) {
+          err = kLobErrRestartOrth;
+          goto finish;
+        }
+        apply_normal(X, bs, AX);
+        form_gram(X, AX, (int)bs);
+        if (!tiny_gep((int)bs)) {
+          err = kLobErrGep;
+          goto finish;
+        }
+        theta_from(bs, (int)bs);
+        continue;
+      }
+
+      // W = R (no preconditioner on the device engine)
+      for (int64_t j = ini; j < bs; j++)
+        copy(col(Rb, j), col(W, j));
+      const int64_t na = bs - ini;
+      for (int64_t t = 0; t < na; t++)
+        copy(col(W, ini + t), col(T1, t));
+      if (!orthonormalize_block(T1, na, d.Yl, nlocked, o.gs_tol, o.gs_reorth != 0, T2)) {
+        for (int64_t j = ini; j < bs; j++)
+          random(col(W, j));
+        for (int64_t j = ini; j < bs; j++)
+          gs_pass(d.Yl, nlocked, col(W, j));
+      } else {
+        for (int64_t t = 0; t < na; t++)
+          copy(col(T1, t), col(W, ini + t));
+      }
+      if (its > 1) {
+        for (int64_t t = 0; t < na; t++)
+          copy(col(P, ini + t), col(T1, t));
+        (void)orthonormalize_block(T1, na, d.Yl, nlocked, o.gs_tol, o.gs_reorth != 0, T2);
+        for (int64_t t = 0; t < na; t++)
+          copy(col(T1, t), col(P, ini + t));
+      }
+      const int64_t np = (its > 1) ? na : 0;
+      const int64_t nv = na + na + np;
+      if (nv == 0)
+        continue;
+      if (o.max_tiny_dim > 0 && nv > o.max_tiny_dim) {
+        err = kLobErrTinyDim;
+        goto finish;
+      }
+      // Z = [X_act | W_act | P_act] (contiguous copy)
+      for (int64_t t = 0; t < na; t++) {
+        copy(col(X, ini + t), col(d.Z, t));
+        copy(col(W, ini + t), col(d.Z, na + t));
+        if (np)
+          copy(col(P, ini + t), col(d.Z, 2 * na + t));
+      }
+      apply_normal(d.Z, nv, d.AZ);
+      form_gram(d.Z, d.AZ, (int)nv);
+      if (!tiny_gep((int)nv)) {
+        err = kLobErrGep;
+        goto finish;
+      }
+      {
+        const int64_t take = na < nv ? na : nv;
+        // P_new = [W P] [Yw; Yp]; X_new = X_act Yx + P_new
+        combine(d.Z + na * ldn, (int)(na + np), d.Ym, (int)nv, (int)na, (int)take, T1);
+        combine(d.Z, (int)na, d.Ym, (int)nv, 0, (int)take, T2);
+        for (int64_t j = 0; j < take; j++)
+          copy(col(T1, j), col(P, ini + j));
+        for (int64_t j = 0; j < take; j++) {
+          double *xo = col(X, ini + j);
+          const double *a = col(T2, j), *b = col(P, ini + j);
+          team_for(tm, n, [&](int64_t i) { xo[i] = a[i] + b[i]; });
+          c.bytes += 24.0 * n;
+          tm.sync();
+        }
+        if (!orthonormalize_block(X + ini * ldn, take, d.Yl, nlocked, o.gs_tol, o.gs_reorth != 0, T1)) {
+          err = kLobErrXSlice;
+          goto finish;
+        }
+      }
+      // full Rayleigh-Ritz for ordering
+      apply_normal(X, bs, AX);
+      form_gram(X, AX, (int)bs);
+      if (!tiny_gep((int)bs)) {
+        err = kLobErrGep;
+        goto finish;
+      }
+      combine(X, (int)bs, d.Ym, (int)bs, 0, (int)bs, T1);
+      for (int64_t j = 0; j < bs; j++)
+        copy(col(T1, j), col(X, j));
+      apply_normal(X, bs, AX);
+      theta_from(bs, (int)bs);
+    }
+    R.converged = (R.locked >= k_target) ? 1 : 0;
+
+    if (nright > 0 && tm.ok()) {
+      const double desired = fmax(o.tol_abs, o.tol_rel * fmax(1.0, R.frob));
+      const double target = fmax(1e-14, fmin(1e-10, 0.01 * desired));
+      if (!polish(d.RN, nright, target, 80))
+        goto finish;
+      for (int64_t i = 0; i < nright; i++) {
+        if (normA(col(d.RN, i), d.ptmp) <= target)
+          continue;
+        (void)sharpen(d.RN, nright, i, target, 120);
+      }
+      mgs(d.RN, nright, 1e-14, true);
+    }
+  finish:
+    tm.sync();
+    if (tm.leader()) {
+      R.n_right = nright;
+      R.status = *(volatile int *)d.status;
+      R.err_code = err;
+      R.spmv = c.spmv;
+      R.spmvT = c.spmvT;
+      R.bytes = c.bytes;
+      R.gram_flops = gram_flops;
+      *d.res = R;
+    }
+  }
+};
+
+__global__ void __launch_bounds__(512) lobpcg_grid_kernel(LobpcgDesc d) {
+  __shared__ TeamShared sh;
+  TeamGrid tm{&sh, d.status, d.gb, d.gpart, 0, 0};
+  LobpcgSolver<TeamGrid> s(tm, d);
+  s.run();
+}
+
+__global__ void __launch_bounds__(512) lobpcg_cta_kernel(const LobpcgDesc *dp) {
+  __shared__ TeamShared sh;
+  const LobpcgDesc &d = *dp;
+  TeamCta tm{&sh, d.status, 0};
+  LobpcgSolver<TeamCta> s(tm, d);
+  s.run();
+}
+
+} // namespace kr

@@ -364,7 +364,3 @@ extern "C" int krans_solve_cyclic(krans_ctx *ctx, const krans_mat *A, krans_rng 
   return rc;
 }
 
-extern "C" int krans_solve_lobpcg(krans_ctx *ctx, const krans_mat *A, krans_rng *rng,
-                                  const krans_lobpcg_opts *opts, const krans_vec *const *initial_block,
-                                  int64_t n_initial, krans_vec **right_out, double *theta_out,
-                                  double *resid_out, krans_lobpcg_result *result);

@@ -1,0 +1,298 @@
+// LOBPCG launch: argument rules of the reference, workspace, team choice.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "kr_internal.h"
+#include "kr_lobpcg.cuh"
+
+namespace kr {
+int grid_blocks_for(krans_ctx *ctx, const void *kernel, int threads);
+
+static inline int64_t rup(int64_t x, int64_t a) { return (x + a - 1) / a * a; }
+
+struct LCarver {
+  size_t off = 0;
+  char *base = nullptr;
+  template <class T> T *take(int64_t count) {
+    off = (size_t)rup((int64_t)off, 256);
+    T *p = base ? (T *)(base + off) : nullptr;
+    off += (size_t)std::max<int64_t>(count, 1) * sizeof(T);
+    return p;
+  }
+};
+
+static size_t lobpcg_layout(int64_t m, int64_t n, int64_t bs, int64_t k, int64_t pmax, int ncta, char *base,
+                            LobpcgDesc *d) {
+  LCarver c;
+  c.base = base;
+  const int64_t ldn = rup(std::max<int64_t>(n, 1), 32), ldm = rup(std::max<int64_t>(m, 1), 32);
+  LobpcgDesc t;
+  memset(&t, 0, sizeof t);
+  t.X = c.take<double>(bs * ldn);
+  t.AX = c.take<double>(bs * ldn);
+  t.Rb = c.take<double>(bs * ldn);
+  t.W = c.take<double>(bs * ldn);
+  t.P = c.take<double>(bs * ldn);
+  t.T1 = c.take<double>(bs * ldn);
+  t.T2 = c.take<double>(bs * ldn);
+  t.Z = c.take<double>(3 * bs * ldn);
+  t.AZ = c.take<double>(3 * bs * ldn);
+  t.Yl = c.take<double>(std::max<int64_t>(k, 1) * ldn);
+  t.RN = c.take<double>(std::max<int64_t>(k, 1) * ldn);
+  t.tmv = c.take<double>(ldm);
+  t.vacc = c.take<double>(ldn);
+  t.theta = c.take<double>(bs);
+  t.th = c.take<double>(pmax);
+  t.S = c.take<double>(pmax * pmax);
+  t.G = c.take<double>(pmax * pmax);
+  t.Ym = c.take<double>(pmax * pmax);
+  t.Sj = c.take<double>(pmax * pmax);
+  t.Li = c.take<double>(pmax * pmax);
+  t.Tm = c.take<double>(pmax * pmax);
+  t.Cm = c.take<double>(pmax * pmax);
+  t.Q = c.take<double>(pmax * pmax);
+  t.eig_cs = c.take<double>(2 * (pmax / 2 + 2));
+  t.eig_pq = c.take<int32_t>(2 * (pmax / 2 + 2));
+  t.eig_ord = c.take<int32_t>(pmax + 4);
+  t.gram_part = c.take<double>((int64_t)ncta * 2 * pmax * pmax);
+  t.theta_out = c.take<double>(std::max<int64_t>(k, 1));
+  t.resid_out = c.take<double>(std::max<int64_t>(k, 1));
+  t.pr = c.take<double>(ldm);
+  t.pg = c.take<double>(ldn);
+  t.ptmp = c.take<double>(ldm);
+  t.Vb = c.take<double>(std::max<int64_t>(k, 1) * ldn);
+  t.D = c.take<double>((k + 2) * ldn);
+  t.Vn = c.take<double>((k + 2) * ldn);
+  t.Zp = c.take<double>((2 * k + 2) * ldn);
+  t.AZp = c.take<double>((2 * k + 2) * ldn);
+  t.sv_av = c.take<double>(ldm);
+  t.sv_t = c.take<double>(ldn);
+  t.sv_d = c.take<double>(ldn);
+  t.sv_ad = c.take<double>(ldm);
+  t.sv_nd = c.take<double>(ldn);
+  t.sv_vn = c.take<double>(ldn);
+  t.status = c.take<int32_t>(1);
+  t.res = c.take<LobpcgDevResult>(1);
+  t.gb = c.take<GridBarrierState>(1);
+  t.gpart = c.take<double>(2 * std::max(ncta, 1) * KR_RED_K);
+  t.flag = c.take<int32_t>(4);
+  t.dflag = c.take<double>(4);
+  if (d) {
+    LobpcgDesc keep = *d;
+    *d = t;
+    d->F = keep.F;
+    d->B = keep.B;
+    d->o = keep.o;
+    d->k_target = keep.k_target;
+    d->bs = keep.bs;
+    d->guards = keep.guards;
+    d->rng = keep.rng;
+    d->initial = keep.initial;
+    d->n_initial = keep.n_initial;
+    d->ldn = ldn;
+    d->ldm = ldm;
+    d->pmax = pmax;
+  }
+  return c.off + 256;
+}
+
+static const char *lobpcg_err_msg(int code) {
+  switch (code) {
+  case kLobErrInitialDependent:
+    return "LOBPCG: initial block is dependent";
+  case kLobErrRestartOrth:
+    return "LOBPCG: restart orthogonalization failed";
+  case kLobErrXSlice:
+    return "LOBPCG: X slice orthonormalization failed";
+  case kLobErrGep:
+    return "LOBPCG tiny GEP: S not SPD (after jitter)";
+  case kLobErrTinyDim:
+    return "LOBPCG: tiny problem too large (nv cap)";
+  default:
+    return "LOBPCG: unknown device error";
+  }
+}
+
+} // namespace kr
+
+using namespace kr;
+
+extern "C" int krans_solve_lobpcg(krans_ctx *ctx, const krans_mat *A, krans_rng *rng,
+                                  const krans_lobpcg_opts *opts, const krans_vec *const *initial_block,
+                                  int64_t n_initial, krans_vec **right_out, double *theta_out,
+                                  double *resid_out, krans_lobpcg_result *result) {
+  KR_CHECK_ARG(ctx && A && rng && opts && result, "krans_solve_lobpcg: NULL argument");
+  KR_CHECK_ARG(A->ctx == ctx && rng->ctx == ctx, "krans_solve_lobpcg: objects of another context");
+  memset(result, 0, sizeof *result);
+  const krans_lobpcg_opts &o = *opts;
+  const int64_t m = A->m, n = A->n;
+  if (n == 0 || m == 0)
+    return KRANS_OK;
+  // k_target rules and argument checks (LOBPCGSolver.cpp:453-476)
+  int64_t k_target = std::max<int64_t>(1, o.nev);
+  if (o.nullity_known >= 0) {
+    KR_CHECK_ARG((int64_t)o.nullity_known <= n, "LOBPCG: nullity_known > n");
+    k_target = o.nullity_known;
+  }
+  if (o.rank_known >= 0) {
+    const int64_t rk = o.rank_known;
+    KR_CHECK_ARG(rk <= n, "LOBPCG: rank_known > n");
+    const int64_t implied = n - rk;
+    KR_CHECK_ARG(!(o.nullity_known >= 0 && implied != k_target),
+                 "LOBPCG: inconsistent rank_known vs nullity_known");
+    if (o.nullity_known < 0)
+      k_target = implied;
+    if (n <= rk) {
+      result->frob_norm_est = 0.0;
+      result->converged_to_target = (k_target == 0);
+      return KRANS_OK;
+    }
+  }
+  int64_t bs = o.block_size > 0 ? o.block_size : std::min<int64_t>(16, std::max<int64_t>(1, k_target));
+  bs = std::min<int64_t>(bs, n);
+  result->block_size = bs;
+  const int64_t guards =
+      (bs == 1) ? 0 : std::min<int64_t>((int64_t)((1.0 - o.restart) * (double)bs + 0.45), bs - 1);
+  KR_CHECK_ARG(bs <= 128, "krans_solve_lobpcg: block_size above 128 is not supported");
+  KR_CHECK_ARG(k_target <= 512, "krans_solve_lobpcg: more than 512 null vectors");
+  if (n_initial > 0)
+    KR_CHECK_ARG(initial_block != nullptr, "krans_solve_lobpcg: initial_block is NULL");
+  for (int64_t i = 0; i < n_initial; i++)
+    KR_CHECK_ARG(initial_block[i] && initial_block[i]->n == n, "krans_solve_lobpcg: initial vector size mismatch");
+  KR_CUDA(cudaSetDevice(ctx->device));
+  std::lock_guard<std::mutex> lk(ctx->mu);
+
+  const int64_t pmax = std::max<int64_t>(3 * bs, 2 * k_target + 2);
+  int team = o.team;
+  if (team == KRANS_TEAM_AUTO)
+    team = (m + n) < 120000 ? KRANS_TEAM_CTA : KRANS_TEAM_GRID;
+  const int threads = 512;
+  const int ncta = team == KRANS_TEAM_GRID ? grid_blocks_for(ctx, (const void *)lobpcg_grid_kernel, threads) : 1;
+
+  LobpcgDesc d;
+  memset(&d, 0, sizeof d);
+  d.F = CsrView{A->m, A->n, A->nnz, A->rp, A->ci, A->v, A->v32, A->lanes};
+  d.B = CsrView{A->n, A->m, A->nnz, A->rpT, A->ciT, A->vT, A->vT32, A->lanesT};
+  d.o = o;
+  d.k_target = k_target;
+  d.bs = bs;
+  d.guards = guards;
+  d.rng = rng->d;
+  d.n_initial = n_initial;
+  const size_t bytes = lobpcg_layout(m, n, bs, k_target, pmax, ncta, nullptr, nullptr);
+  char *ws = nullptr;
+  int rc = dev_alloc(ctx, (void **)&ws, bytes);
+  if (rc != KRANS_OK)
+    return rc;
+  double **d_init = nullptr;
+  std::vector<double *> hinit;
+  for (int64_t i = 0; i < n_initial; i++)
+    hinit.push_back(initial_block[i]->d);
+  cudaStream_t s = ctx->stream;
+  cudaError_t e = cudaSuccess;
+  if (n_initial > 0) {
+    e = cudaMalloc(&d_init, sizeof(double *) * (size_t)n_initial);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(d_init, hinit.data(), sizeof(double *) * (size_t)n_initial, cudaMemcpyHostToDevice, s);
+  }
+  d.initial = d_init;
+  lobpcg_layout(m, n, bs, k_target, pmax, ncta, ws, &d);
+  LobpcgDesc *d_desc = nullptr;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  if (e == cudaSuccess)
+    e = cudaMemsetAsync(d.status, 0, 4, s);
+  if (e == cudaSuccess)
+    e = cudaMemsetAsync(d.gb, 0, sizeof(GridBarrierState), s);
+  if (e == cudaSuccess)
+    e = cudaMemsetAsync(d.res, 0, sizeof(LobpcgDevResult), s);
+  if (e == cudaSuccess)
+    e = cudaEventRecord(e0, s);
+  if (e == cudaSuccess) {
+    if (team == KRANS_TEAM_GRID) {
+      void *args[] = {(void *)&d};
+      e = cudaLaunchCooperativeKernel((const void *)lobpcg_grid_kernel, dim3(ncta), dim3(threads), args, 0, s);
+    } else {
+      e = cudaMalloc(&d_desc, sizeof(LobpcgDesc));
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync(d_desc, &d, sizeof d, cudaMemcpyHostToDevice, s);
+      if (e == cudaSuccess) {
+        lobpcg_cta_kernel<<<1, threads, 0, s>>>(d_desc);
+        e = cudaGetLastError();
+      }
+    }
+  }
+  if (e == cudaSuccess)
+    e = cudaEventRecord(e1, s);
+  LobpcgDevResult R;
+  memset(&R, 0, sizeof R);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(&R, d.res, sizeof R, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess)
+    e = cudaStreamSynchronize(s);
+  float ms = 0.f;
+  if (e == cudaSuccess)
+    cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (d_desc)
+    cudaFree(d_desc);
+  if (d_init)
+    cudaFree(d_init);
+  if (e != cudaSuccess) {
+    dev_free(ctx, ws, bytes);
+    return cuda_fail(e, "lobpcg launch", __FILE__, __LINE__);
+  }
+  if (R.status != KRANS_OK) {
+    dev_free(ctx, ws, bytes);
+    set_error("LOBPCG: device status %d (a bounded device wait gave up)", R.status);
+    return R.status;
+  }
+  result->iters = R.iters;
+  result->locked = R.locked;
+  result->frob_norm_est = R.frob;
+  result->accept_threshold = R.accept;
+  result->best_unaccepted_residual = R.best_unaccepted;
+  result->converged_to_target = R.converged;
+  result->spmv = R.spmv;
+  result->spmvT = R.spmvT;
+  result->algo_bytes = R.bytes;
+  result->gram_flops = R.gram_flops;
+  result->device_ms = ms;
+  if (R.err_code != kLobErrNone) {
+    dev_free(ctx, ws, bytes);
+    set_error("%s", lobpcg_err_msg(R.err_code));
+    return KRANS_ERR_RUNTIME;
+  }
+  KR_CHECK_ARG(right_out || R.n_right == 0, "krans_solve_lobpcg: right_out is NULL");
+  std::vector<double> th((size_t)std::max<int64_t>(R.n_right, 1)), rs((size_t)std::max<int64_t>(R.n_right, 1));
+  if (R.n_right > 0) {
+    e = cudaMemcpyAsync(th.data(), d.theta_out, 8 * (size_t)R.n_right, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(rs.data(), d.resid_out, 8 * (size_t)R.n_right, cudaMemcpyDeviceToHost, s);
+  }
+  for (int64_t i = 0; i < R.n_right && e == cudaSuccess && rc == KRANS_OK; i++) {
+    krans_vec *v = nullptr;
+    rc = krans_vec_create(ctx, n, &v);
+    if (rc == KRANS_OK) {
+      e = cudaMemcpyAsync(v->d, d.RN + i * d.ldn, (size_t)n * 8, cudaMemcpyDeviceToDevice, s);
+      right_out[i] = v;
+      result->n_right = i + 1;
+    }
+  }
+  if (e == cudaSuccess)
+    e = cudaStreamSynchronize(s);
+  dev_free(ctx, ws, bytes);
+  if (e != cudaSuccess)
+    return cuda_fail(e, "lobpcg results", __FILE__, __LINE__);
+  if (theta_out)
+    for (int64_t i = 0; i < R.n_right; i++)
+      theta_out[i] = th[i];
+  if (resid_out)
+    for (int64_t i = 0; i < R.n_right; i++)
+      resid_out[i] = rs[i];
+  return rc;
+}
