@@ -5,7 +5,7 @@
 #include <cstring>
 #include <random>
 
-#include "kr_cyclic.cuh"
+#include "kr_device.cuh"
 #include "kr_internal.h"
 
 namespace kr {

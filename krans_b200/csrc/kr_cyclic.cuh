@@ -24,45 +24,6 @@
 
 namespace kr {
 
-struct CsrView {
-  int64_t rows, cols, nnz;
-  const int32_t *rp, *ci;
-  const double *v64;
-  const float *v32;
-  int lanes; // threads per row in the SpMV
-};
-
-struct CyclicDevResult {
-  int64_t n_found;
-  int64_t restarts, krylov_steps_total, cg_solves, cg_maxit_hits, spmv, spmvT;
-  double frob, bytes;
-  int32_t converged;
-  int32_t status;
-};
-
-struct CyclicDesc {
-  CsrView F, B; // F: the run's operator (rows m, cols n); B: its transpose
-  krans_cyclic_opts o;
-  int64_t k_target, ncv;
-  int32_t trans_run; // 1 for the left-space run (counts swap)
-  RngState *rng;
-  const double *initial_right; // n doubles or nullptr
-  double *basis;               // k_target x ldn (output, row i = vector i)
-  void *Y, *X, *wx, *wy;       // KT storage
-  double *y0, *v, *vp, *best_v, *tn; // n-vectors
-  double *tmv, *wm, *r, *p, *Ap;     // m-vectors
-  double *alpha, *beta;              // ncv + 2
-  double *Tb, *Vt, *sv;              // tiny problem
-  int32_t *ord;
-  double *eig_cs;
-  int32_t *eig_pq, *eig_ord;
-  int64_t ldn, ldm, ldb, cap; // ldb: stride of the basis rows
-  int32_t *status;
-  CyclicDevResult *res;
-  GridBarrierState *gb;
-  double *gpart;
-};
-
 // counters kept identically by every thread (uniform control flow)
 struct Counters {
   int64_t spmv = 0, spmvT = 0, cg_solves = 0, cg_maxit_hits = 0, steps = 0, restarts = 0;
@@ -141,7 +102,7 @@ template <class Team, class KT> struct CyclicSolver {
   }
 
   // two classical Gram-Schmidt passes against the accepted basis (double)
-  KR_DEV void gs2_basis(double *v) {
+  __device__ __noinline__ void gs2_basis(double *v) {
     if (nb == 0)
       return;
     for (int pass = 0; pass < 2; pass++) {
@@ -161,7 +122,7 @@ template <class Team, class KT> struct CyclicSolver {
     tm.sync();
   }
 
-  KR_DEV double fro_est() {
+  __device__ __noinline__ double fro_est() {
     const int samples = d.o.frob_samples > 1 ? d.o.frob_samples : 1;
     double sum2 = 0.0;
     for (int s = 0; s < samples; s++) {
@@ -173,16 +134,24 @@ template <class Team, class KT> struct CyclicSolver {
   }
 
   // CG on (F F^T) w = rhs (CyclicLanczosSolver.cpp:48-113), no preconditioner.
-  KR_DEV int64_t cg(const double *rhs, double *w, int64_t maxit, double rel_tol, double bd_tol,
+  __device__ __noinline__ int64_t cg(const double *rhs, double *w, int64_t maxit, double rel_tol, double bd_tol,
                     double *rnorm_out) {
     double *r = d.r, *p = d.p, *Ap = d.Ap, *tn = d.tn;
     double rr = 0.0;
-    team_for(tm, m, [&](int64_t i) {
-      const double x = rhs[i];
-      w[i] = 0.0;
-      r[i] = x;
-      p[i] = x;
-      rr += x * x;
+    team_for4(tm, m, [&](const int64_t *ix, int cnt) {
+      double xv[4];
+#pragma unroll
+      for (int u = 0; u < 4; u++)
+        if (u < cnt)
+          xv[u] = rhs[ix[u]];
+#pragma unroll
+      for (int u = 0; u < 4; u++)
+        if (u < cnt) {
+          w[ix[u]] = 0.0;
+          r[ix[u]] = xv[u];
+          p[ix[u]] = xv[u];
+          rr += xv[u] * xv[u];
+        }
     });
     rr = tm.sum1(rr);
     c.bytes += 32.0 * m;
@@ -213,11 +182,24 @@ template <class Team, class KT> struct CyclicSolver {
         break;
       const double alpha = rz / pap;
       double rzn = 0.0;
-      team_for(tm, m, [&](int64_t i) {
-        w[i] += alpha * p[i];
-        const double ri = r[i] - alpha * Ap[i];
-        r[i] = ri;
-        rzn += ri * ri;
+      team_for4(tm, m, [&](const int64_t *ix, int cnt) {
+        double pv[4], wv[4], rv[4], av[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+          if (u < cnt) {
+            pv[u] = p[ix[u]];
+            wv[u] = w[ix[u]];
+            rv[u] = r[ix[u]];
+            av[u] = Ap[ix[u]];
+          }
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+          if (u < cnt) {
+            w[ix[u]] = wv[u] + alpha * pv[u];
+            const double ri = rv[u] - alpha * av[u];
+            r[ix[u]] = ri;
+            rzn += ri * ri;
+          }
       });
       rzn = tm.sum1(rzn);
       c.bytes += 40.0 * m;
@@ -230,7 +212,19 @@ template <class Team, class KT> struct CyclicSolver {
       }
       const double beta = rzn / fmax(1e-300, rz);
       rz = rzn;
-      team_for(tm, m, [&](int64_t i) { p[i] = p[i] * beta + r[i]; });
+      team_for4(tm, m, [&](const int64_t *ix, int cnt) {
+        double pv[4], rv[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+          if (u < cnt) {
+            pv[u] = p[ix[u]];
+            rv[u] = r[ix[u]];
+          }
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+          if (u < cnt)
+            p[ix[u]] = pv[u] * beta + rv[u];
+      });
       c.bytes += 24.0 * m;
       tm.sync();
     }
@@ -239,7 +233,7 @@ template <class Team, class KT> struct CyclicSolver {
   }
 
   // try_project_random_to_nullspace (CyclicLanczosSolver.cpp:140-214)
-  KR_DEV bool try_project_random(double accept) {
+  __device__ __noinline__ bool try_project_random(double accept) {
     double *v = d.v, *tmv = d.tmv, *wm = d.wm, *tn = d.tn;
     random(v);
     // single GS pass vs basis
@@ -301,7 +295,7 @@ template <class Team, class KT> struct CyclicSolver {
   // Build and solve the projected problem on the leader block. Writes the
   // candidate coefficient matrix (over the Y vectors) into d.Vt, their
   // ordering into d.ord; returns the number of candidates (uniform).
-  KR_DEV int tiny_problem(int l, double beta_last, int ny) {
+  __device__ __noinline__ int tiny_problem(int l, double beta_last, int ny) {
     const double tau = d.o.target_tau;
     const bool harmonic = d.o.use_harmonic != 0;
     const bool split = harmonic && tau == 0.0;
@@ -424,7 +418,7 @@ template <class Team, class KT> struct CyclicSolver {
     return *(volatile double *)&d.Vt[(size_t)jb * l + 2 * t];
   }
 
-  KR_DEV void run() {
+  __device__ __noinline__ void run() {
     const krans_cyclic_opts &o = d.o;
     KT *Y = (KT *)d.Y, *X = (KT *)d.X, *wx = (KT *)d.wx, *wy = (KT *)d.wy;
     const int64_t ldn = d.ldn, ldm = d.ldm;
@@ -571,11 +565,23 @@ template <class Team, class KT> struct CyclicSolver {
         if (threadIdx.x < (unsigned)ny_used)
           tm.sh->h[threadIdx.x] = coef(split, l, jb, threadIdx.x);
         __syncthreads();
-        team_for(tm, n, [&](int64_t i) {
-          double acc = 0.0;
-          for (int q = 0; q < ny_used; q++)
-            acc += tm.sh->h[q] * (double)Y[(int64_t)q * ldn + i];
-          v[i] = acc;
+        team_for4(tm, n, [&](const int64_t *ix, int cnt) {
+          double acc[4] = {0.0, 0.0, 0.0, 0.0};
+          for (int q = 0; q < ny_used; q++) {
+            const double hq = tm.sh->h[q];
+            const KT *yq = Y + (int64_t)q * ldn;
+            double yv[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++)
+              yv[u] = u < cnt ? (double)yq[ix[u]] : 0.0;
+#pragma unroll
+            for (int u = 0; u < 4; u++)
+              acc[u] += hq * yv[u];
+          }
+#pragma unroll
+          for (int u = 0; u < 4; u++)
+            if (u < cnt)
+              v[ix[u]] = acc[u];
         });
         c.bytes += (double)(ny_used * sizeof(KT) + 8) * n;
         tm.sync();
@@ -697,27 +703,6 @@ __global__ void __launch_bounds__(512) cyclic_grid_kernel(CyclicDesc d) {
   TeamGrid tm{&sh, d.status, d.gb, d.gpart, 0, 0};
   CyclicSolver<TeamGrid, KT> s(tm, d);
   s.run();
-}
-
-template <class KT>
-__global__ void __launch_bounds__(512) cyclic_cta_kernel(const CyclicDesc *descs, int count,
-                                                         int *queue) {
-  __shared__ TeamShared sh;
-  __shared__ int s_item;
-  for (;;) {
-    if (threadIdx.x == 0)
-      s_item = atomicAdd(queue, 1);
-    __syncthreads();
-    const int item = s_item;
-    __syncthreads();
-    if (item >= count)
-      break;
-    const CyclicDesc &d = descs[item];
-    TeamCta tm{&sh, d.status, 0};
-    CyclicSolver<TeamCta, KT> s(tm, d);
-    s.run();
-    __syncthreads();
-  }
 }
 
 } // namespace kr

@@ -10,14 +10,18 @@
 // so a solve gives bit-identical results alone and inside a batch.
 #pragma once
 
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
 #include "../../include/krans_cuda.h"
+#include "kr_types.cuh"
 
 #define KR_DEV __device__ __forceinline__
 #define KR_MAX_WARPS 32
+#ifndef KR_RED_K
 #define KR_RED_K 8 // values per fused team reduction
+#endif
 
 namespace kr {
 
@@ -34,18 +38,12 @@ KR_DEV uint64_t globaltimer_ns() {
 // (the longest legitimate wait is a serial section on the leader block).
 constexpr uint64_t kBarrierTimeoutNs = 8ull * 1000ull * 1000ull * 1000ull;
 
-struct GridBarrierState {
-  unsigned int count;
-  unsigned int gen;
-  int error; // sticky: once set, barriers return at once and solvers unwind
-  int pad;
-};
-
 // Per-block shared memory used by the team primitives.
 struct TeamShared {
   double red[2][KR_MAX_WARPS * KR_RED_K]; // double-buffered warp partials
   double bc[KR_RED_K];                    // broadcast slots (grid reductions)
   double h[160];                          // Gram-Schmidt coefficients
+  double cpart[2][KR_RED_K];              // cluster reductions: this block's partials
   int ibuf[64];                           // small integer scratch
 };
 
@@ -198,6 +196,66 @@ struct TeamGrid {
   KR_DEV void publish() { sync(); }
 };
 
+// A thread-block cluster (up to 16 blocks on distinct SMs of one GPC) as a
+// team: hardware cluster barrier, reductions through distributed shared
+// memory (each block publishes its partial in its own shared memory, every
+// block sums the partials of ranks 0..size-1 in order).
+struct TeamCluster {
+  TeamShared *sh;
+  int *err;
+  int buf;
+  int cbuf;
+  unsigned rank, csize;
+  KR_DEV int64_t tid() const { return (int64_t)rank * blockDim.x + threadIdx.x; }
+  KR_DEV int64_t nthreads() const { return (int64_t)csize * blockDim.x; }
+  KR_DEV int64_t warp_id() const { return tid() >> 5; }
+  KR_DEV int64_t nwarps() const { return nthreads() >> 5; }
+  KR_DEV bool lead_cta() const { return rank == 0; }
+  KR_DEV bool leader() const { return rank == 0 && threadIdx.x == 0; }
+  KR_DEV int cta_rank() const { return (int)rank; }
+  KR_DEV int ncta() const { return (int)csize; }
+  KR_DEV bool ok() const { return *(volatile int *)err == 0; }
+  KR_DEV void sync() { cooperative_groups::this_cluster().sync(); }
+  template <int K> KR_DEV void sum(double (&v)[K]) {
+    block_sum<K>(sh, buf, v);
+    if (threadIdx.x == 0) {
+#pragma unroll
+      for (int k = 0; k < K; k++)
+        sh->cpart[cbuf][k] = v[k];
+    }
+    cooperative_groups::cluster_group cl = cooperative_groups::this_cluster();
+    cl.sync();
+    if (threadIdx.x < 32) {
+      const unsigned lane = threadIdx.x;
+      double mine[K];
+      const double *peer = cl.map_shared_rank(&sh->cpart[cbuf][0], lane < csize ? lane : 0);
+#pragma unroll
+      for (int k = 0; k < K; k++)
+        mine[k] = lane < csize ? peer[k] : 0.0;
+#pragma unroll
+      for (int k = 0; k < K; k++) {
+        double t = 0.0;
+        for (unsigned r = 0; r < csize; r++)
+          t += __shfl_sync(0xffffffffu, mine[k], r);
+        if (lane == 0)
+          sh->bc[k] = t;
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < K; k++)
+      v[k] = sh->bc[k];
+    __syncthreads();
+    cbuf ^= 1;
+  }
+  KR_DEV double sum1(double x) {
+    double v[1] = {x};
+    sum<1>(v);
+    return v[0];
+  }
+  KR_DEV void publish() { sync(); }
+};
+
 // ---------------------------------------------------------------------------
 // Element-wise team loops (grid-stride over the team's threads)
 // ---------------------------------------------------------------------------
@@ -214,6 +272,7 @@ template <class Team, class TX, class TY>
 KR_DEV double team_dot(Team &tm, int64_t len, const TX *x, const TY *y) {
   double s = 0.0;
   const int64_t nt = tm.nthreads();
+#pragma unroll 4
   for (int64_t i = tm.tid(); i < len; i += nt)
     s += to_d(x[i]) * to_d(y[i]);
   return tm.sum1(s);
@@ -240,6 +299,7 @@ KR_DEV void team_multidot(Team &tm, int64_t len, const TS *S, int64_t ld, int ns
     for (int k = 0; k < KR_RED_K; k++)
       acc[k] = 0.0;
     const int qn = min(KR_RED_K, ns - q0);
+#pragma unroll 4
     for (int64_t i = tm.tid(); i < len; i += nt) {
       const double wi = to_d(w[i]);
 #pragma unroll
@@ -259,11 +319,47 @@ template <class Team, class TS, class TW>
 KR_DEV void team_multi_axpy(Team &tm, int64_t len, const TS *S, int64_t ld, int ns,
                             const double *coef, TW *w) {
   const int64_t nt = tm.nthreads();
-  for (int64_t i = tm.tid(); i < len; i += nt) {
+  int64_t i = tm.tid();
+  for (; i + 3 * nt < len; i += 4 * nt) {
+    double acc[4];
+#pragma unroll
+    for (int u = 0; u < 4; u++)
+      acc[u] = to_d(w[i + u * nt]);
+    for (int q = 0; q < ns; q++) {
+      const double cq = coef[q];
+      const TS *sq = S + (int64_t)q * ld + i;
+      double sv[4];
+#pragma unroll
+      for (int u = 0; u < 4; u++)
+        sv[u] = to_d(sq[u * nt]);
+#pragma unroll
+      for (int u = 0; u < 4; u++)
+        acc[u] -= sv[u] * cq;
+    }
+#pragma unroll
+    for (int u = 0; u < 4; u++)
+      w[i + u * nt] = (TW)acc[u];
+  }
+  for (; i < len; i += nt) {
     double acc = to_d(w[i]);
     for (int q = 0; q < ns; q++)
       acc -= to_d(S[(int64_t)q * ld + i]) * coef[q];
     w[i] = (TW)acc;
+  }
+}
+
+// Streams `len` elements with each thread handling 4 indices per step; the
+// functor gets (index array, count) and must load all inputs before storing.
+template <class Team, class F> KR_DEV void team_for4(Team &tm, int64_t len, F f) {
+  const int64_t nt = tm.nthreads();
+  int64_t i = tm.tid();
+  for (; i + 3 * nt < len; i += 4 * nt) {
+    const int64_t idx[4] = {i, i + nt, i + 2 * nt, i + 3 * nt};
+    f(idx, 4);
+  }
+  for (; i < len; i += nt) {
+    const int64_t idx[4] = {i, i, i, i};
+    f(idx, 1);
   }
 }
 
@@ -280,23 +376,65 @@ template <class Team, class VT, class XT, class Epi>
 KR_DEV void team_spmv(Team &tm, int64_t rows, const int32_t *__restrict__ rp,
                       const int32_t *__restrict__ ci, const VT *__restrict__ val,
                       const XT *__restrict__ x, int lanes, Epi epi) {
+  // Each warp walks R row groups at once: all row pointers, then all
+  // (column, value) pairs, then all x gathers are issued before the FMAs, so
+  // a thread keeps R independent loads in flight. Lane `sub` of a row sums
+  // the entries b+sub, b+sub+lanes, ... in order, then a fixed butterfly
+  // combines the lanes: the result does not depend on R or on the team.
   using Acc = typename AccOf<VT>::T;
+  constexpr int R = 4;
   const int lane = threadIdx.x & 31;
-  const int sub = lane & (lanes - 1);
-  const int rows_per_warp = 32 / lanes;
+  const int sub = lane & (lanes - 1), grp = lane / lanes;
+  const int rpw = 32 / lanes;
+  const int64_t chunk = (int64_t)rpw * R;
   const int64_t nw = tm.nwarps();
-  for (int64_t base = tm.warp_id() * rows_per_warp; base < rows; base += nw * rows_per_warp) {
-    const int64_t i = base + lane / lanes;
-    Acc s = Acc(0);
-    if (i < rows) {
-      const int32_t b = __ldg(rp + i), e = __ldg(rp + i + 1);
-      for (int32_t k = b + sub; k < e; k += lanes)
-        s += (Acc)__ldg(val + k) * (Acc)x[__ldg(ci + k)];
+  for (int64_t base = tm.warp_id() * chunk; base < rows; base += nw * chunk) {
+    int32_t b[R], e[R];
+#pragma unroll
+    for (int u = 0; u < R; u++) {
+      const int64_t i = base + (int64_t)u * rpw + grp;
+      b[u] = 0;
+      e[u] = 0;
+      if (i < rows) {
+        b[u] = __ldg(rp + i) + sub;
+        e[u] = __ldg(rp + i + 1);
+      }
     }
-    for (int o = lanes >> 1; o > 0; o >>= 1)
-      s += __shfl_xor_sync(0xffffffffu, s, o);
-    if (i < rows && sub == 0)
-      epi(i, s);
+    Acc s[R];
+#pragma unroll
+    for (int u = 0; u < R; u++)
+      s[u] = Acc(0);
+    for (int32_t j = 0;; j += lanes) {
+      int32_t c[R];
+      VT v[R];
+      bool ok[R], more = false;
+#pragma unroll
+      for (int u = 0; u < R; u++) {
+        const int32_t k = b[u] + j;
+        ok[u] = k < e[u];
+        more |= (k + lanes) < e[u];
+        c[u] = ok[u] ? __ldg(ci + k) : 0;
+        v[u] = ok[u] ? __ldg(val + k) : VT(0);
+      }
+      XT xv[R];
+#pragma unroll
+      for (int u = 0; u < R; u++)
+        xv[u] = ok[u] ? x[c[u]] : XT(0);
+#pragma unroll
+      for (int u = 0; u < R; u++)
+        if (ok[u])
+          s[u] += (Acc)v[u] * (Acc)xv[u];
+      if (!more)
+        break;
+    }
+#pragma unroll
+    for (int u = 0; u < R; u++) {
+      for (int o = lanes >> 1; o > 0; o >>= 1)
+        s[u] += __shfl_xor_sync(0xffffffffu, s[u], o);
+      const int64_t i = base + (int64_t)u * rpw + grp;
+      if (i < rows && sub == 0)
+        epi(i, s[u]);
+    }
   }
 }
 
@@ -309,18 +447,6 @@ __host__ __device__ inline double spmv_bytes(int64_t r, int64_t c, int64_t z, in
 // ---------------------------------------------------------------------------
 // Random normal vectors
 // ---------------------------------------------------------------------------
-// State of one factory stream. Layout of the MT part equals the CPU oracle's.
-struct RngState {
-  uint32_t mt[624];
-  int32_t idx;
-  int32_t has_saved;
-  double saved;
-  uint64_t philox_key;
-  uint64_t philox_ctr;
-  int32_t mode;
-  int32_t pad;
-};
-
 KR_DEV uint32_t mt_temper(uint32_t y) {
   y ^= y >> 11;
   y ^= (y << 7) & 0x9d2c5680u;

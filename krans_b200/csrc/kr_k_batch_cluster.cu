@@ -1,0 +1,49 @@
+// Kernel TU: cyclic Lanczos with one thread-block cluster per request.
+#include <algorithm>
+
+#include "kr_batch.cuh"
+#include "kr_internal.h"
+
+namespace kr {
+
+static const void *cl_kernel(bool mixed) {
+  return mixed ? (const void *)cyclic_batch_cluster_kernel<float> : (const void *)cyclic_batch_cluster_kernel<double>;
+}
+
+static cudaLaunchConfig_t cl_config(int nclusters, int csize, cudaStream_t s, cudaLaunchAttribute *at) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(nclusters * csize);
+  cfg.blockDim = dim3(512);
+  cfg.stream = s;
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = csize;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cfg;
+}
+
+int cyclic_batch_cluster_max(bool mixed, int csize, int sms) {
+  if (csize > 8)
+    cudaFuncSetAttribute(cl_kernel(mixed), cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+  cudaLaunchAttribute at[1];
+  cudaLaunchConfig_t cfg = cl_config(64, csize, nullptr, at);
+  int maxc = 0;
+  if (cudaOccupancyMaxActiveClusters(&maxc, cl_kernel(mixed), &cfg) != cudaSuccess || maxc < 1) {
+    cudaGetLastError();
+    maxc = std::max(1, sms / (2 * csize));
+  }
+  return maxc;
+}
+
+cudaError_t launch_cyclic_batch_cluster(bool mixed, int nclusters, int csize, cudaStream_t s,
+                                        const CyclicRequestDev *reqs, int count, int *queue, char *ws, size_t stride) {
+  cudaLaunchAttribute at[1];
+  cudaLaunchConfig_t cfg = cl_config(nclusters, csize, s, at);
+  if (mixed)
+    return cudaLaunchKernelEx(&cfg, cyclic_batch_cluster_kernel<float>, reqs, count, queue, ws, stride);
+  return cudaLaunchKernelEx(&cfg, cyclic_batch_cluster_kernel<double>, reqs, count, queue, ws, stride);
+}
+
+} // namespace kr

@@ -1,0 +1,27 @@
+// Kernel TU: cyclic Lanczos with one thread block per request (persistent,
+// device work queue). Also serves single small requests.
+#include "kr_batch.cuh"
+#include "kr_internal.h"
+
+namespace kr {
+
+int cyclic_batch_cta_per_sm(bool mixed) {
+  const void *k = mixed ? (const void *)cyclic_batch_kernel<float> : (const void *)cyclic_batch_kernel<double>;
+  int per_sm = 1;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, 512, 0) != cudaSuccess || per_sm < 1) {
+    cudaGetLastError();
+    per_sm = 1;
+  }
+  return per_sm;
+}
+
+cudaError_t launch_cyclic_batch_cta(bool mixed, int grid, cudaStream_t s, const CyclicRequestDev *reqs, int count,
+                                    int *queue, char *ws, size_t stride) {
+  if (mixed)
+    cyclic_batch_kernel<float><<<grid, 512, 0, s>>>(reqs, count, queue, ws, stride);
+  else
+    cyclic_batch_kernel<double><<<grid, 512, 0, s>>>(reqs, count, queue, ws, stride);
+  return cudaGetLastError();
+}
+
+} // namespace kr

@@ -19,56 +19,6 @@
 
 namespace kr {
 
-struct LobpcgDevResult {
-  int64_t n_right, iters, locked, block_size;
-  double frob, accept, best_unaccepted;
-  int32_t converged, status;
-  int32_t err_code, pad;
-  int64_t spmv, spmvT;
-  double bytes, gram_flops;
-};
-
-// error codes of the reference's throws (reported as KRANS_ERR_RUNTIME)
-enum LobpcgErr {
-  kLobErrNone = 0,
-  kLobErrInitialDependent = 1, // "LOBPCG: initial block is dependent"
-  kLobErrRestartOrth = 2,      // "LOBPCG: restart orthogonalization failed"
-  kLobErrXSlice = 3,           // "LOBPCG: X slice orthonormalization failed"
-  kLobErrGep = 4,              // "LOBPCG tiny GEP: S not SPD (after jitter)"
-  kLobErrTinyDim = 5,          // "LOBPCG: tiny problem too large (nv cap)"
-};
-
-struct LobpcgDesc {
-  CsrView F, B; // A (m x n) and A^T
-  krans_lobpcg_opts o;
-  int64_t k_target, bs, guards;
-  RngState *rng;
-  double *const *initial; // n_initial device vectors (or nullptr)
-  int64_t n_initial;
-  // blocks (column-major, ld = ldn)
-  double *X, *AX, *Rb, *W, *P, *T1, *T2, *Z, *AZ;
-  double *Yl, *RN; // locked set and output basis (k_target columns)
-  double *tmv, *vacc;
-  double *theta, *th;
-  // small dense matrices (pmax x pmax)
-  double *S, *G, *Ym, *Sj, *Li, *Tm, *Cm, *Q;
-  double *eig_cs;
-  int32_t *eig_pq, *eig_ord;
-  double *gram_part;
-  double *theta_out, *resid_out; // k_target
-  // polish scratch
-  double *pr, *pg, *ptmp;              // m, n, m
-  double *Vb, *D, *Vn, *Zp, *AZp;      // k, k+2, k, 2k+2, 2k+2 columns
-  double *sv_av, *sv_t, *sv_d, *sv_ad, *sv_nd, *sv_vn; // sharpen scratch
-  int64_t ldn, ldm, pmax;
-  int32_t *status;
-  LobpcgDevResult *res;
-  GridBarrierState *gb;
-  double *gpart;
-  int32_t *flag; // uniform scalar broadcast slot (leader writes, all read)
-  double *dflag;
-};
-
 template <class Team> struct LobpcgSolver {
   Team &tm;
   const LobpcgDesc &d;
@@ -136,7 +86,7 @@ template <class Team> struct LobpcgSolver {
   }
   // x -= sum_q <x, B_q> B_q over nb columns (one classical pass); when
   // skip_zero, coefficients that are exactly 0 are dropped (project_out).
-  KR_DEV void gs_pass(const double *Bk, int64_t nb, double *x) {
+  __device__ __noinline__ void gs_pass(const double *Bk, int64_t nb, double *x) {
     if (nb <= 0)
       return;
     for (int64_t q0 = 0; q0 < nb; q0 += 128) {
@@ -148,7 +98,7 @@ template <class Team> struct LobpcgSolver {
     }
   }
   // same against an arbitrary list of columns given by index set of a block
-  KR_DEV void gs_pass_excl(const double *Bk, int64_t nb, int64_t excl, double *x) {
+  __device__ __noinline__ void gs_pass_excl(const double *Bk, int64_t nb, int64_t excl, double *x) {
     // project x against columns q != excl, one at a time in the group form
     for (int64_t q0 = 0; q0 < nb; q0 += 128) {
       const int cnt = (int)imin64(128, nb - q0);
@@ -163,7 +113,7 @@ template <class Team> struct LobpcgSolver {
   }
 
   // MGS with optional reorth (GramSchmidt.cpp:55-82) on k columns of block V.
-  KR_DEV bool mgs(double *V, int64_t k, double tol, bool reorth) {
+  __device__ __noinline__ bool mgs(double *V, int64_t k, double tol, bool reorth) {
     for (int64_t i = 0; i < k; i++) {
       double *vi = col(V, i);
       gs_pass(V, i, vi);
@@ -185,7 +135,7 @@ template <class Team> struct LobpcgSolver {
   // orthonormalize_block (LOBPCGSolver.cpp:137-160): project each column vs
   // basis and normalise (in place), then MGS on a copy in `scratch`, copied
   // back only on success.
-  KR_DEV bool orthonormalize_block(double *Xb, int64_t k, const double *basis, int64_t nb, double tol,
+  __device__ __noinline__ bool orthonormalize_block(double *Xb, int64_t k, const double *basis, int64_t nb, double tol,
                                    bool reorth, double *scratch) {
     for (int64_t i = 0; i < k; i++) {
       double *xi = col(Xb, i);
@@ -204,14 +154,14 @@ template <class Team> struct LobpcgSolver {
     return true;
   }
 
-  KR_DEV void apply_normal(const double *Zb, int64_t k, double *AZb) {
+  __device__ __noinline__ void apply_normal(const double *Zb, int64_t k, double *AZb) {
     for (int64_t j = 0; j < k; j++) {
       mulA(col((double *)Zb, j), d.tmv);
       mulAT(d.tmv, col(AZb, j));
     }
   }
 
-  KR_DEV void form_gram(const double *Zb, const double *AZb, int p) {
+  __device__ __noinline__ void form_gram(const double *Zb, const double *AZb, int p) {
     team_gram2(tm, n, Zb, AZb, ldn, p, d.S, d.G, d.gram_part);
     gram_flops += 2.0 * 2.0 * (double)n * p * p;
     c.bytes += 2.0 * 8.0 * n * p;
@@ -219,13 +169,13 @@ template <class Team> struct LobpcgSolver {
 
   // solve_tiny_gep (LOBPCGSolver.cpp:88-119) on the leader block; theta in
   // d.th, eigenvectors in d.Ym (ld p). Returns false if S is not SPD.
-  KR_DEV bool tiny_gep(int p) {
+  __device__ __noinline__ bool tiny_gep(int p) {
     if (tm.lead_cta())
       gep_block(p);
     tm.publish();
     return *(volatile int32_t *)d.flag == 0;
   }
-  KR_DEV void gep_block(int p) {
+  __device__ __noinline__ void gep_block(int p) {
     double *S = d.S, *G = d.G;
     // symmetrize
     for (int e = threadIdx.x; e < p * p; e += blockDim.x) {
@@ -287,7 +237,7 @@ template <class Team> struct LobpcgSolver {
   }
 
   // out[i] = sum_{j<zc} Y(roff+j, i) Z_j for i < q (Y has leading dim ldy)
-  KR_DEV void combine(const double *Zb, int zc, const double *Y, int ldy, int roff, int q, double *out) {
+  __device__ __noinline__ void combine(const double *Zb, int zc, const double *Y, int ldy, int roff, int q, double *out) {
     team_combine(tm, n, Zb, ldn, zc, Y, ldy, roff, q, out);
     c.bytes += (double)(zc + q) * 8.0 * n;
     tm.sync();
@@ -306,7 +256,7 @@ template <class Team> struct LobpcgSolver {
   KR_DEV double theta_of(int64_t j) const { return *(volatile double *)&d.theta[j]; }
 
   // ---- two_vec_rr_sharpen (LOBPCGSolver.cpp:199-278) ------------------------
-  KR_DEV bool sharpen(double *V, int64_t k, int64_t idx, double target, int max_iters) {
+  __device__ __noinline__ bool sharpen(double *V, int64_t k, int64_t idx, double target, int max_iters) {
     if (idx >= k)
       return true;
     double *Av = d.sv_av, *t = d.sv_t, *dd = d.sv_d, *Ad = d.sv_ad, *Nd = d.sv_nd, *vn = d.sv_vn;
@@ -370,7 +320,7 @@ template <class Team> struct LobpcgSolver {
   }
 
   // ---- block_rr_polish (LOBPCGSolver.cpp:286-440) ---------------------------
-  KR_DEV bool polish(double *V, int64_t k, double target, int max_sweeps) {
+  __device__ __noinline__ bool polish(double *V, int64_t k, double target, int max_sweeps) {
     if (k == 0)
       return true;
     double *r = d.pr, *g = d.pg, *tmp = d.ptmp;
@@ -474,7 +424,7 @@ template <class Team> struct LobpcgSolver {
     return true;
   }
 
-  KR_DEV void run() {
+  __device__ __noinline__ void run() {
     const krans_lobpcg_opts &o = d.o;
     const int64_t bs = d.bs, k_target = d.k_target, guards = d.guards;
     LobpcgDevResult R;
@@ -714,13 +664,16 @@ template <class Team> struct LobpcgSolver {
   }
 };
 
+#ifdef KR_LOBPCG_GRID_KERNEL
 __global__ void __launch_bounds__(512) lobpcg_grid_kernel(LobpcgDesc d) {
   __shared__ TeamShared sh;
   TeamGrid tm{&sh, d.status, d.gb, d.gpart, 0, 0};
   LobpcgSolver<TeamGrid> s(tm, d);
   s.run();
 }
+#endif
 
+#ifdef KR_LOBPCG_CTA_KERNEL
 __global__ void __launch_bounds__(512) lobpcg_cta_kernel(const LobpcgDesc *dp) {
   __shared__ TeamShared sh;
   const LobpcgDesc &d = *dp;
@@ -728,5 +681,6 @@ __global__ void __launch_bounds__(512) lobpcg_cta_kernel(const LobpcgDesc *dp) {
   LobpcgSolver<TeamCta> s(tm, d);
   s.run();
 }
+#endif
 
 } // namespace kr

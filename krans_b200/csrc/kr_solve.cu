@@ -6,101 +6,15 @@
 #include <numeric>
 #include <vector>
 
-#include "kr_cyclic.cuh"
 #include "kr_internal.h"
+#include "kr_types.cuh"
 
 namespace kr {
 
-static inline int64_t round_up(int64_t x, int64_t a) { return (x + a - 1) / a * a; }
-
-// Carves one device allocation into 256-byte aligned arrays.
-struct Carver {
-  size_t off = 0;
-  char *base = nullptr;
-  template <class T> T *take(int64_t count) {
-    off = (size_t)round_up((int64_t)off, 256);
-    T *p = base ? (T *)(base + off) : nullptr;
-    off += (size_t)std::max<int64_t>(count, 1) * sizeof(T);
-    return p;
-  }
-};
-
-struct CyclicPlan {
-  int64_t m, n, k_target, ncv, ldn, ldm, ldb, cap;
-  int ksz; // bytes of the Krylov storage type
-  int grid_blocks;
-};
+static inline int64_t round_up(int64_t x, int64_t a) { return kr_round_up(x, a); }
 
 // Lay out (or, with base == nullptr, size) the workspace of one run.
-static size_t cyclic_layout(const CyclicPlan &p, char *base, CyclicDesc *d) {
-  Carver c;
-  c.base = base;
-  CyclicDesc t;
-  memset(&t, 0, sizeof t);
-  t.Y = c.take<char>(p.cap * p.ldn * p.ksz);
-  t.X = c.take<char>(p.cap * p.ldm * p.ksz);
-  t.wx = c.take<char>(p.ldm * p.ksz);
-  t.wy = c.take<char>(p.ldn * p.ksz);
-  t.basis = c.take<double>(std::max<int64_t>(p.k_target, 1) * p.ldb);
-  t.y0 = c.take<double>(p.ldn);
-  t.v = c.take<double>(p.ldn);
-  t.vp = c.take<double>(p.ldn);
-  t.best_v = c.take<double>(p.ldn);
-  t.tn = c.take<double>(p.ldn);
-  t.tmv = c.take<double>(p.ldm);
-  t.wm = c.take<double>(p.ldm);
-  t.r = c.take<double>(p.ldm);
-  t.p = c.take<double>(p.ldm);
-  t.Ap = c.take<double>(p.ldm);
-  t.alpha = c.take<double>(p.ncv + 2);
-  t.beta = c.take<double>(p.ncv + 2);
-  t.Tb = c.take<double>((p.ncv + 1) * p.ncv);
-  t.Vt = c.take<double>(p.ncv * p.ncv);
-  t.sv = c.take<double>(p.ncv + 1);
-  t.ord = c.take<int32_t>(p.ncv + 2);
-  t.eig_cs = c.take<double>(p.ncv * p.ncv + 2 * p.ncv + 4);
-  t.eig_pq = c.take<int32_t>(p.ncv + 4);
-  t.eig_ord = c.take<int32_t>(p.ncv + 4);
-  t.status = c.take<int32_t>(1);
-  t.res = c.take<CyclicDevResult>(1);
-  t.gb = c.take<GridBarrierState>(1);
-  t.gpart = c.take<double>(2 * std::max(p.grid_blocks, 1) * KR_RED_K);
-  if (d) {
-    d->Y = t.Y;
-    d->X = t.X;
-    d->wx = t.wx;
-    d->wy = t.wy;
-    d->basis = t.basis;
-    d->y0 = t.y0;
-    d->v = t.v;
-    d->vp = t.vp;
-    d->best_v = t.best_v;
-    d->tn = t.tn;
-    d->tmv = t.tmv;
-    d->wm = t.wm;
-    d->r = t.r;
-    d->p = t.p;
-    d->Ap = t.Ap;
-    d->alpha = t.alpha;
-    d->beta = t.beta;
-    d->Tb = t.Tb;
-    d->Vt = t.Vt;
-    d->sv = t.sv;
-    d->ord = t.ord;
-    d->eig_cs = t.eig_cs;
-    d->eig_pq = t.eig_pq;
-    d->eig_ord = t.eig_ord;
-    d->status = t.status;
-    d->res = t.res;
-    d->gb = t.gb;
-    d->gpart = t.gpart;
-    d->ldn = p.ldn;
-    d->ldm = p.ldm;
-    d->ldb = p.ldb;
-    d->cap = p.cap;
-  }
-  return c.off + 256;
-}
+static size_t cyclic_layout(const CyclicPlan &p, char *base, CyclicDesc *d) { return cyclic_carve(p, base, d); }
 
 static CsrView view_of(const krans_mat *A, bool trans) {
   CsrView v;
@@ -131,22 +45,14 @@ static int cyclic_targets(const krans_cyclic_opts &o, int64_t m, int64_t n, int6
   return 0;
 }
 
-int grid_blocks_for(krans_ctx *ctx, const void *kernel, int threads) {
-  int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0) != cudaSuccess ||
-      per_sm < 1)
-    per_sm = 1;
-  per_sm = std::min(per_sm, 2);
-  return ctx->sms * per_sm;
-}
-
 struct RunOut {
   CyclicDevResult r;
   double ms;
 };
 
-// One find_right_nullspace run on the device; basis rows land in `basis_dev`
-// (stride ldb) owned by the workspace, copied into new vectors by the caller.
+// One find_right_nullspace run on the device (a grid team, or one thread
+// block through the persistent batched kernel with a single request); the
+// basis rows are copied into new vectors owned by the caller.
 static int run_cyclic(krans_ctx *ctx, const krans_mat *A, bool trans, krans_rng *rng,
                       const krans_cyclic_opts &o, const double *init_right, int64_t k_target,
                       int64_t ncv, std::vector<krans_vec *> &found, RunOut *out) {
@@ -161,9 +67,10 @@ static int run_cyclic(krans_ctx *ctx, const krans_mat *A, bool trans, krans_rng 
   int team = o.team;
   if (team == KRANS_TEAM_AUTO)
     team = (F.rows + F.cols) < 120000 ? KRANS_TEAM_CTA : KRANS_TEAM_GRID;
-  const void *gk = mixed ? (const void *)cyclic_grid_kernel<float> : (const void *)cyclic_grid_kernel<double>;
-  const int threads_grid = 512, threads_cta = 512;
+  const bool grid = team == KRANS_TEAM_GRID;
+  const int threads = 512;
   CyclicPlan p;
+  memset(&p, 0, sizeof p);
   p.m = F.rows;
   p.n = F.cols;
   p.k_target = k_target;
@@ -173,61 +80,85 @@ static int run_cyclic(krans_ctx *ctx, const krans_mat *A, bool trans, krans_rng 
   p.ldb = p.ldn;
   p.cap = ncv / 2 + 2;
   p.ksz = mixed ? 4 : 8;
-  p.grid_blocks = team == KRANS_TEAM_GRID ? grid_blocks_for(ctx, gk, threads_grid) : 1;
-  const size_t bytes = cyclic_layout(p, nullptr, nullptr);
+  p.grid_blocks = grid ? cyclic_grid_blocks(ctx, mixed, threads) : 1;
+  p.own_basis = grid ? 1 : 0;
+  // one allocation: solver workspace, basis, request record and counters
+  char *slot = nullptr;
+  double *basis = nullptr, *d_mr = nullptr;
+  CyclicRequestDev *d_req = nullptr;
+  CyclicDevResult *d_res = nullptr;
+  int32_t *d_status = nullptr;
+  int *d_queue = nullptr;
+  auto layout = [&](char *base) {
+    Carver c;
+    c.base = base;
+    slot = c.take<char>((int64_t)cyclic_carve(p, nullptr, nullptr));
+    basis = c.take<double>(std::max<int64_t>(k_target, 1) * p.ldb);
+    d_req = c.take<CyclicRequestDev>(1);
+    d_res = c.take<CyclicDevResult>(1);
+    d_status = c.take<int32_t>(1);
+    d_mr = c.take<double>(1);
+    d_queue = c.take<int>(1);
+    return c.off + 256;
+  };
+  const size_t bytes = layout(nullptr);
   char *ws = nullptr;
   int rc = dev_alloc(ctx, (void **)&ws, bytes);
   if (rc != KRANS_OK)
     return rc;
-  CyclicDesc d;
-  memset(&d, 0, sizeof d);
-  cyclic_layout(p, ws, &d);
-  d.F = F;
-  d.B = B;
-  d.o = o;
-  d.k_target = k_target;
-  d.ncv = ncv;
-  d.trans_run = trans ? 1 : 0;
-  d.rng = rng->d;
-  d.initial_right = init_right;
+  layout(ws);
   cudaStream_t s = ctx->stream;
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
-  CyclicDesc *d_desc = nullptr;
-  int *d_queue = nullptr;
-  cudaError_t e = cudaMemsetAsync(d.status, 0, 4, s);
+  cudaError_t e = cudaMemsetAsync(d_res, 0, sizeof(CyclicDevResult), s);
   if (e == cudaSuccess)
-    e = cudaMemsetAsync(d.gb, 0, sizeof(GridBarrierState), s);
+    e = cudaMemsetAsync(d_status, 0, 4, s);
   if (e == cudaSuccess)
-    e = cudaMemsetAsync(d.res, 0, sizeof(CyclicDevResult), s);
+    e = cudaMemsetAsync(d_queue, 0, 4, s);
+  CyclicDesc d;
+  CyclicRequestDev q;
+  if (grid) {
+    memset(&d, 0, sizeof d);
+    cyclic_carve(p, slot, &d);
+    d.F = F;
+    d.B = B;
+    d.o = o;
+    d.k_target = k_target;
+    d.ncv = ncv;
+    d.trans_run = trans ? 1 : 0;
+    d.rng = rng->d;
+    d.initial_right = init_right;
+    d.status = d_status;
+    d.res = d_res;
+    if (e == cudaSuccess)
+      e = cudaMemsetAsync(d.gb, 0, sizeof(GridBarrierState), s);
+  } else {
+    memset(&q, 0, sizeof q);
+    q.F = F;
+    q.B = B;
+    q.o = o;
+    q.plan = p;
+    q.rng = rng->d;
+    q.basis = basis;
+    q.res = d_res;
+    q.status = d_status;
+    q.max_resid = d_mr;
+    q.initial_right = init_right;
+    q.trivial = 0;
+    q.trans_run = trans ? 1 : 0;
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(d_req, &q, sizeof q, cudaMemcpyHostToDevice, s);
+  }
   if (e == cudaSuccess)
     e = cudaEventRecord(e0, s);
-  if (e == cudaSuccess) {
-    if (team == KRANS_TEAM_GRID) {
-      void *args[] = {(void *)&d};
-      e = cudaLaunchCooperativeKernel(gk, dim3(p.grid_blocks), dim3(threads_grid), args, 0, s);
-    } else {
-      e = cudaMalloc(&d_desc, sizeof(CyclicDesc));
-      if (e == cudaSuccess)
-        e = cudaMalloc(&d_queue, sizeof(int));
-      if (e == cudaSuccess)
-        e = cudaMemcpyAsync(d_desc, &d, sizeof d, cudaMemcpyHostToDevice, s);
-      if (e == cudaSuccess)
-        e = cudaMemsetAsync(d_queue, 0, sizeof(int), s);
-      if (e == cudaSuccess) {
-        if (mixed)
-          cyclic_cta_kernel<float><<<1, threads_cta, 0, s>>>(d_desc, 1, d_queue);
-        else
-          cyclic_cta_kernel<double><<<1, threads_cta, 0, s>>>(d_desc, 1, d_queue);
-        e = cudaGetLastError();
-      }
-    }
-  }
+  if (e == cudaSuccess)
+    e = grid ? launch_cyclic_grid(mixed, d, p.grid_blocks, threads, s)
+             : launch_cyclic_batch_cta(mixed, 1, s, d_req, 1, d_queue, slot, 0);
   if (e == cudaSuccess)
     e = cudaEventRecord(e1, s);
   if (e == cudaSuccess)
-    e = cudaMemcpyAsync(&out->r, d.res, sizeof(CyclicDevResult), cudaMemcpyDeviceToHost, s);
+    e = cudaMemcpyAsync(&out->r, d_res, sizeof(CyclicDevResult), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess)
     e = cudaStreamSynchronize(s);
   float ms = 0.f;
@@ -236,10 +167,6 @@ static int run_cyclic(krans_ctx *ctx, const krans_mat *A, bool trans, krans_rng 
   out->ms = ms;
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  if (d_desc)
-    cudaFree(d_desc);
-  if (d_queue)
-    cudaFree(d_queue);
   if (e != cudaSuccess) {
     dev_free(ctx, ws, bytes);
     return cuda_fail(e, "cyclic solve launch", __FILE__, __LINE__);
@@ -249,12 +176,13 @@ static int run_cyclic(krans_ctx *ctx, const krans_mat *A, bool trans, krans_rng 
     set_error("cyclic solve: device status %d (a bounded device wait gave up)", out->r.status);
     return out->r.status;
   }
+  const double *bsrc = grid ? d.basis : basis;
   rc = KRANS_OK;
   for (int64_t i = 0; i < out->r.n_found && rc == KRANS_OK; i++) {
     krans_vec *v = nullptr;
     rc = krans_vec_create(ctx, p.n, &v);
     if (rc == KRANS_OK) {
-      e = cudaMemcpyAsync(v->d, d.basis + i * p.ldb, (size_t)p.n * 8, cudaMemcpyDeviceToDevice, s);
+      e = cudaMemcpyAsync(v->d, bsrc + i * p.ldb, (size_t)p.n * 8, cudaMemcpyDeviceToDevice, s);
       if (e != cudaSuccess)
         rc = cuda_fail(e, "basis copy", __FILE__, __LINE__);
       found.push_back(v);

@@ -5,10 +5,9 @@
 #include <vector>
 
 #include "kr_internal.h"
-#include "kr_lobpcg.cuh"
+#include "kr_types.cuh"
 
 namespace kr {
-int grid_blocks_for(krans_ctx *ctx, const void *kernel, int threads);
 
 static inline int64_t rup(int64_t x, int64_t a) { return (x + a - 1) / a * a; }
 
@@ -169,7 +168,7 @@ extern "C" int krans_solve_lobpcg(krans_ctx *ctx, const krans_mat *A, krans_rng 
   if (team == KRANS_TEAM_AUTO)
     team = (m + n) < 120000 ? KRANS_TEAM_CTA : KRANS_TEAM_GRID;
   const int threads = 512;
-  const int ncta = team == KRANS_TEAM_GRID ? grid_blocks_for(ctx, (const void *)lobpcg_grid_kernel, threads) : 1;
+  const int ncta = team == KRANS_TEAM_GRID ? lobpcg_grid_blocks(ctx, threads) : 1;
 
   LobpcgDesc d;
   memset(&d, 0, sizeof d);
@@ -211,20 +210,13 @@ extern "C" int krans_solve_lobpcg(krans_ctx *ctx, const krans_mat *A, krans_rng 
     e = cudaMemsetAsync(d.res, 0, sizeof(LobpcgDevResult), s);
   if (e == cudaSuccess)
     e = cudaEventRecord(e0, s);
-  if (e == cudaSuccess) {
-    if (team == KRANS_TEAM_GRID) {
-      void *args[] = {(void *)&d};
-      e = cudaLaunchCooperativeKernel((const void *)lobpcg_grid_kernel, dim3(ncta), dim3(threads), args, 0, s);
-    } else {
-      e = cudaMalloc(&d_desc, sizeof(LobpcgDesc));
-      if (e == cudaSuccess)
-        e = cudaMemcpyAsync(d_desc, &d, sizeof d, cudaMemcpyHostToDevice, s);
-      if (e == cudaSuccess) {
-        lobpcg_cta_kernel<<<1, threads, 0, s>>>(d_desc);
-        e = cudaGetLastError();
-      }
-    }
+  if (e == cudaSuccess && team != KRANS_TEAM_GRID) {
+    e = cudaMalloc(&d_desc, sizeof(LobpcgDesc));
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(d_desc, &d, sizeof d, cudaMemcpyHostToDevice, s);
   }
+  if (e == cudaSuccess)
+    e = launch_lobpcg(team == KRANS_TEAM_GRID, d, d_desc, ncta, threads, s);
   if (e == cudaSuccess)
     e = cudaEventRecord(e1, s);
   LobpcgDevResult R;
