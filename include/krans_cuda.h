@@ -95,6 +95,23 @@ int krans_vec_fill(krans_vec *v, double value);                          /* set_
 int krans_vec_copy(krans_vec *dst, const krans_vec *src);                /* copy_from */
 int krans_vec_clone(const krans_vec *src, krans_vec **out);              /* clone */
 
+/* Allocation-free dot product (no counterpart in the reference). For callers
+ * that cannot call cudaMalloc: runtimes that give out device memory only from
+ * their own pre-planned pool, and code that must not synchronize the device
+ * (cudaFree, and often cudaMalloc, synchronize implicitly). Computes
+ * *result = x . y for device arrays x, y of n doubles into a device double,
+ * enqueued on `stream` (a cudaStream_t; NULL = the legacy default stream) of
+ * the current device, without allocating anything and without a context.
+ * Scratch comes from a file-scope device array of KRANS_NOALLOC_DOT_MAX_BLOCKS
+ * doubles (128 KiB, held by every GPU that loads the library until exit); n
+ * above KRANS_NOALLOC_DOT_MAX_N is rejected with KRANS_ERR_INVALID_ARGUMENT.
+ * The first call on a device looks up the array's address (make it before any
+ * stream capture). Calls that overlap on the GPU share the array and race. */
+#define KRANS_NOALLOC_DOT_PER_BLOCK 2048LL
+#define KRANS_NOALLOC_DOT_MAX_BLOCKS 16384LL
+#define KRANS_NOALLOC_DOT_MAX_N (KRANS_NOALLOC_DOT_PER_BLOCK * KRANS_NOALLOC_DOT_MAX_BLOCKS)
+int krans_vec_dot_noalloc(const double *x, const double *y, int64_t n, double *result, void *stream);
+
 /* y <- A x (trans = 0) or y <- A^T x (trans = 1): multiply / multiply_transpose.
  * precision: 0 = FP64 values, 1 = FP32 values with FP32 accumulation. */
 int krans_spmv(const krans_mat *A, int trans, const krans_vec *x, krans_vec *y);

@@ -128,6 +128,7 @@ SIGNATURES = {
     "krans_vec_fill": [P, D],
     "krans_vec_copy": [P, P],
     "krans_vec_clone": [P, PP],
+    "krans_vec_dot_noalloc": [P, P, I64, P, P],
     "krans_spmv": [P, I, P, P],
     "krans_spmv_ex": [P, I, I, P, P],
     "krans_rng_create": [P, C.c_uint32, I, PP],
