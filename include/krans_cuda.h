@@ -179,6 +179,7 @@ typedef struct krans_cyclic_result {
   int64_t spmv, spmvT;       /* operator applications (CountingMatrixAdapter) */
   double algo_bytes;         /* algorithmic HBM bytes of the solve */
   double device_ms;          /* device time of the solve kernel(s) */
+  double phase_ms[4];        /* device time in Golub-Kahan+reorth, tiny SVD, CG polish, rest */
 } krans_cyclic_result;
 
 typedef struct krans_lobpcg_opts {
@@ -259,7 +260,8 @@ typedef struct krans_request_result {
   double frob_norm_est;
   double max_residual;       /* max ||A u||_2 over the returned basis (FP64) */
   double algo_bytes;
-  double queue_ms, device_ms, latency_ms; /* serving only */
+  double queue_ms, device_ms, latency_ms; /* see krans_solve_batch / krans_poll */
+  double phase_ms[4];        /* device time in Golub-Kahan+reorth, tiny SVD, CG polish, rest */
 } krans_request_result;
 
 /* Solve `count` cyclic requests in one persistent launch (one thread block

@@ -55,7 +55,7 @@ class CyclicResultC(C.Structure):
                 ("converged_to_target", C.c_int32), ("status", C.c_int32),
                 ("cg_solves", C.c_int64), ("cg_maxit_hits", C.c_int64),
                 ("spmv", C.c_int64), ("spmvT", C.c_int64), ("algo_bytes", C.c_double),
-                ("device_ms", C.c_double)]
+                ("device_ms", C.c_double), ("phase_ms", C.c_double * 4)]
 
 
 class LobpcgOpts(C.Structure):
@@ -87,7 +87,8 @@ class RequestResult(C.Structure):
                 ("cg_solves", C.c_int64), ("cg_maxit_hits", C.c_int64),
                 ("spmv", C.c_int64), ("spmvT", C.c_int64), ("frob_norm_est", C.c_double),
                 ("max_residual", C.c_double), ("algo_bytes", C.c_double),
-                ("queue_ms", C.c_double), ("device_ms", C.c_double), ("latency_ms", C.c_double)]
+                ("queue_ms", C.c_double), ("device_ms", C.c_double), ("latency_ms", C.c_double),
+                ("phase_ms", C.c_double * 4)]
 
 
 class ServerOpts(C.Structure):
@@ -154,12 +155,13 @@ _RESTYPE = {"krans_last_error": C.c_char_p, "krans_version": C.c_char_p}
 _lib = None
 
 
-def load(path: str = LIB_PATH):
-    """Load the CUDA library. Fails loudly when it is missing: there is no
-    CPU fallback behind this API."""
+def load(path: str = None):
+    """Load the CUDA library (KRANS_B200_LIB overrides the in-tree path).
+    Fails loudly when it is missing: there is no CPU fallback behind this API."""
     global _lib
     if _lib is not None:
         return _lib
+    path = path or os.environ.get("KRANS_B200_LIB", LIB_PATH)
     if not os.path.exists(path):
         raise ImportError(f"{path} not built; run `python -m krans_b200.build` "
                           "(the engine has no CPU fallback)")

@@ -326,6 +326,7 @@ class CyclicLanczosResult:
     spmvT: int = 0
     algo_bytes: float = 0.0
     device_ms: float = 0.0
+    phase_ms: tuple = (0.0, 0.0, 0.0, 0.0)
 
 
 @dataclass
@@ -405,7 +406,8 @@ def find_nullspace_cyclic_lanczos_ex(A: CudaCsrMatrixAdapter, vf: CudaVectorFact
         restarts=res.restarts, krylov_steps_total=res.krylov_steps_total,
         frob_norm_est=res.frob_norm_est, converged_to_target=bool(res.converged_to_target),
         cg_solves=res.cg_solves, cg_maxit_hits=res.cg_maxit_hits, spmv=res.spmv,
-        spmvT=res.spmvT, algo_bytes=res.algo_bytes, device_ms=res.device_ms)
+        spmvT=res.spmvT, algo_bytes=res.algo_bytes, device_ms=res.device_ms,
+        phase_ms=tuple(res.phase_ms))
     return R
 
 

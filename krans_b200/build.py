@@ -15,10 +15,12 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
-LIB = os.path.join(HERE, "libkrans_cuda.so")
-BUILD_DIR = os.path.join(HERE, "_build")
+LIB = os.environ.get("KRANS_B200_BUILD_LIB", os.path.join(HERE, "libkrans_cuda.so"))
+BUILD_DIR = os.environ.get("KRANS_B200_BUILD_DIR", os.path.join(HERE, "_build"))
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC = os.environ.get("NVCC", "nvcc")
+# extra nvcc flags for tuning builds (e.g. "-DKR_SPMV_ROWS=8")
+EXTRA = os.environ.get("KRANS_NVCC_FLAGS", "").split()
 
 
 def _sources():
@@ -46,7 +48,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     for src in _sources():
         obj = os.path.join(BUILD_DIR, os.path.basename(src) + ".o")
         cmd = [NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr",
-               "--extended-lambda", "-Xcompiler", "-fPIC,-O3", "-c", src, "-o", obj]
+               "--extended-lambda", "-Xcompiler", "-fPIC,-O3", *EXTRA, "-c", src, "-o", obj]
         if verbose:
             cmd.insert(1, "-Xptxas=-v")
         procs.append((src, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)))

@@ -99,8 +99,8 @@ struct BatchLaunch {
                    "krans_solve_batch: mixed precision needs matrices created with KRANS_CSR_FP32");
       const krans_mat *A = r.A;
       CyclicRequestDev &q = hreq[pos];
-      q.F = CsrView{A->m, A->n, A->nnz, A->rp, A->ci, A->v, A->v32, A->lanes};
-      q.B = CsrView{A->n, A->m, A->nnz, A->rpT, A->ciT, A->vT, A->vT32, A->lanesT};
+      q.F = CsrView{A->m, A->n, A->nnz, A->rp, A->ci, A->v, A->v32, A->lanes, A->ulen};
+      q.B = CsrView{A->n, A->m, A->nnz, A->rpT, A->ciT, A->vT, A->vT32, A->lanesT, A->ulenT};
       q.o = r.opts;
       q.o.team = KRANS_TEAM_CTA;
       int64_t kt = (r.opts.nullity_known >= 0) ? (int64_t)r.opts.nullity_known : r.opts.k;
@@ -144,11 +144,11 @@ struct BatchLaunch {
     grid = n_small > 0 ? std::max(1, std::min(n_small, ctx->sms * per_sm)) : 0;
     nclusters = 0;
     if (n_large > 0) {
+      // one cluster launch fills the GPU; its blocks take the small requests
+      // after the large queue is empty (one small-request slot per block)
       const int maxc = cyclic_batch_cluster_max(mixed, csize, ctx->sms);
-      nclusters = std::max(1, std::min(n_large, maxc));
-      // leave room for the CTA-team launch when both run
-      if (n_small > 0 && grid > 0)
-        grid = std::max(1, std::min(grid, ctx->sms * per_sm - nclusters * csize));
+      nclusters = std::max(1, maxc);
+      grid = nclusters * csize;
     }
     meta_bytes = (size_t)n * (sizeof(CyclicRequestDev) + sizeof(CyclicDevResult) + 4 + 8 + sizeof(RngState)) +
                  4096;
@@ -207,24 +207,14 @@ struct BatchLaunch {
     if (e == cudaSuccess)
       e = cudaEventRecord(ev0, s);
     char *ws_small = ws, *ws_large = ws + (size_t)grid * ws_stride;
-    if (e == cudaSuccess && n_large > 0) {
-      // clusters on an auxiliary stream, concurrent with the CTA-team launch
-      e = cudaStreamCreateWithFlags(&aux, cudaStreamNonBlocking);
-      if (e == cudaSuccess)
-        e = cudaEventCreateWithFlags(&evj, cudaEventDisableTiming);
-      if (e == cudaSuccess)
-        e = cudaStreamWaitEvent(aux, ev0, 0);
-      if (e == cudaSuccess)
-        e = launch_cyclic_batch_cluster(precision == KRANS_PREC_MIXED, nclusters, csize, aux, d_reqs, n_large,
-                                        d_queue, ws_large, stride_L);
-      if (e == cudaSuccess)
-        e = cudaEventRecord(evj, aux);
+    const bool mixed = precision == KRANS_PREC_MIXED;
+    if (e == cudaSuccess) {
+      if (n_large > 0)
+        e = launch_cyclic_batch_cluster(mixed, nclusters, csize, s, d_reqs, n_large, d_queue, ws_large, stride_L,
+                                        d_reqs + n_large, count - n_large, d_queue + 1, ws_small, ws_stride);
+      else
+        e = launch_cyclic_batch_cta(mixed, grid, s, d_reqs, count, d_queue + 1, ws_small, ws_stride);
     }
-    if (e == cudaSuccess && count - n_large > 0)
-      e = launch_cyclic_batch_cta(precision == KRANS_PREC_MIXED, grid, s, d_reqs + n_large, count - n_large,
-                                  d_queue + 1, ws_small, ws_stride);
-    if (e == cudaSuccess && n_large > 0)
-      e = cudaStreamWaitEvent(s, evj, 0);
     if (e == cudaSuccess)
       e = cudaEventRecord(ev1, s);
     if (e == cudaSuccess)
@@ -279,6 +269,8 @@ struct BatchLaunch {
     out->frob_norm_est = r.frob;
     out->max_residual = h_mr[pos];
     out->algo_bytes = r.bytes;
+    for (int q = 0; q < 4; q++)
+      out->phase_ms[q] = r.phase_ms[q];
   }
 
   void release() {

@@ -6,6 +6,10 @@
 
 #include "kr_cyclic.cuh"
 
+#ifndef KR_BATCH_MIN_BLOCKS
+#define KR_BATCH_MIN_BLOCKS 1 // resident blocks per SM the register budget is sized for
+#endif
+
 namespace kr {
 
 template <class Team> KR_DEV double team_max_residual(Team &tm, const CsrView &F, const double *basis,
@@ -14,15 +18,56 @@ template <class Team> KR_DEV double team_max_residual(Team &tm, const CsrView &F
   for (int64_t i = 0; i < nf; i++) {
     const double *u = basis + i * ldb;
     double s2 = 0.0;
-    team_spmv(tm, F.rows, F.rp, F.ci, F.v64, u, F.lanes, [&](int64_t, double s) { s2 += s * s; });
+    csr_mv(tm, F, F.v64, u, [&](int64_t, double s) { s2 += s * s; });
     mr = fmax(mr, sqrt(tm.sum1(s2)));
   }
   return mr;
 }
 
+// One request on one thread block, with its workspace laid out in `slot`.
 template <class KT>
-__global__ void __launch_bounds__(512) cyclic_batch_kernel(const CyclicRequestDev *reqs, int count, int *queue,
-                                                           char *ws, size_t ws_stride) {
+__device__ __noinline__ void run_cta_request(TeamShared *sh, CyclicDesc *dp, const CyclicRequestDev &rq,
+                                             char *slot) {
+  CyclicDesc &d = *dp;
+  if (threadIdx.x == 0) {
+    memset(&d, 0, sizeof d);
+    cyclic_carve(rq.plan, slot, &d);
+    d.F = rq.F;
+    d.B = rq.B;
+    d.o = rq.o;
+    d.k_target = rq.plan.k_target;
+    d.ncv = rq.plan.ncv;
+    d.trans_run = rq.trans_run;
+    d.rng = rq.rng;
+    d.initial_right = rq.initial_right;
+    d.basis = rq.basis;
+    d.ldb = rq.plan.ldb;
+    d.status = rq.status;
+    d.res = rq.res;
+    rq.res->t_begin = globaltimer_ns();
+  }
+  __syncthreads();
+  if (!rq.trivial) {
+    TeamCta tm{sh, d.status, 0};
+    CyclicSolver<TeamCta, KT> s(tm, d);
+    s.run();
+    __syncthreads();
+    const int64_t nf = *(volatile int64_t *)&d.res->n_found;
+    const double mr = team_max_residual(tm, d.F, d.basis, d.ldb, nf);
+    if (threadIdx.x == 0)
+      *rq.max_resid = mr;
+  }
+  if (threadIdx.x == 0)
+    rq.res->t_end = globaltimer_ns();
+  __syncthreads();
+}
+
+// Persistent kernel, one thread block per request: blocks take requests from
+// the device queue until it is empty. Block b owns workspace slot b.
+template <class KT>
+__global__ void __launch_bounds__(512, KR_BATCH_MIN_BLOCKS) cyclic_batch_kernel(const CyclicRequestDev *reqs,
+                                                                               int count, int *queue, char *ws,
+                                                                               size_t ws_stride) {
   __shared__ TeamShared sh;
   __shared__ CyclicDesc d;
   __shared__ int s_item;
@@ -32,66 +77,40 @@ __global__ void __launch_bounds__(512) cyclic_batch_kernel(const CyclicRequestDe
       s_item = atomicAdd(queue, 1);
     __syncthreads();
     const int item = s_item;
+    __syncthreads();
     if (item >= count)
       break;
-    const CyclicRequestDev &rq = reqs[item];
-    if (threadIdx.x == 0) {
-      memset(&d, 0, sizeof d);
-      cyclic_carve(rq.plan, slot, &d);
-      d.F = rq.F;
-      d.B = rq.B;
-      d.o = rq.o;
-      d.k_target = rq.plan.k_target;
-      d.ncv = rq.plan.ncv;
-      d.trans_run = rq.trans_run;
-      d.rng = rq.rng;
-      d.initial_right = rq.initial_right;
-      d.basis = rq.basis;
-      d.ldb = rq.plan.ldb;
-      d.status = rq.status;
-      d.res = rq.res;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0)
-      rq.res->t_begin = globaltimer_ns();
-    if (!rq.trivial) {
-      TeamCta tm{&sh, d.status, 0};
-      CyclicSolver<TeamCta, KT> s(tm, d);
-      s.run();
-      __syncthreads();
-      const int64_t nf = *(volatile int64_t *)&d.res->n_found;
-      const double mr = team_max_residual(tm, d.F, d.basis, d.ldb, nf);
-      if (threadIdx.x == 0)
-        *rq.max_resid = mr;
-    }
-    if (threadIdx.x == 0)
-      rq.res->t_end = globaltimer_ns();
-    __syncthreads();
+    run_cta_request<KT>(&sh, &d, reqs[item], slot);
   }
 }
 
-// Same as cyclic_batch_kernel with a thread-block cluster per request: the
-// cluster's rank 0 takes the next request; every block lays out the same
-// slot descriptor; the solve runs on a TeamCluster.
+// Persistent kernel over a batch with large and small requests. Each
+// thread-block cluster first takes large requests (a TeamCluster per request,
+// the cluster's rank 0 draws from the large queue); once that queue is empty,
+// every block of every cluster keeps going on its own with small requests
+// (one-block teams), so no SM idles while work of either kind remains.
+// Cluster c owns large slot c; block b owns small slot b.
 template <class KT>
-__global__ void __launch_bounds__(512) cyclic_batch_cluster_kernel(const CyclicRequestDev *reqs, int count,
-                                                                   int *queue, char *ws, size_t ws_stride) {
+__global__ void __launch_bounds__(512, KR_BATCH_MIN_BLOCKS)
+    cyclic_batch_cluster_kernel(const CyclicRequestDev *reqs_large, int n_large, int *queue_large, char *ws_large,
+                                size_t stride_large, const CyclicRequestDev *reqs_small, int n_small,
+                                int *queue_small, char *ws_small, size_t stride_small) {
   __shared__ TeamShared sh;
   __shared__ CyclicDesc d;
   __shared__ int s_item;
   cooperative_groups::cluster_group cl = cooperative_groups::this_cluster();
   const unsigned rank = cl.block_rank(), csize = cl.num_blocks();
-  char *slot = ws + (size_t)(blockIdx.x / csize) * ws_stride;
+  char *slot = ws_large + (size_t)(blockIdx.x / csize) * stride_large;
   int cbuf = 0;
   for (;;) {
     if (rank == 0 && threadIdx.x == 0)
-      s_item = atomicAdd(queue, 1);
+      s_item = atomicAdd(queue_large, 1);
     cl.sync();
     const int item = *cl.map_shared_rank(&s_item, 0);
     cl.sync();
-    if (item >= count)
+    if (item >= n_large)
       break;
-    const CyclicRequestDev &rq = reqs[item];
+    const CyclicRequestDev &rq = reqs_large[item];
     if (threadIdx.x == 0) {
       memset(&d, 0, sizeof d);
       cyclic_carve(rq.plan, slot, &d);
@@ -125,6 +144,18 @@ __global__ void __launch_bounds__(512) cyclic_batch_cluster_kernel(const CyclicR
     if (rank == 0 && threadIdx.x == 0)
       rq.res->t_end = globaltimer_ns();
     cl.sync();
+  }
+  // small requests, block by block (no cluster-wide synchronisation below)
+  char *cslot = ws_small + (size_t)blockIdx.x * stride_small;
+  for (;;) {
+    if (threadIdx.x == 0)
+      s_item = atomicAdd(queue_small, 1);
+    __syncthreads();
+    const int item = s_item;
+    __syncthreads();
+    if (item >= n_small)
+      break;
+    run_cta_request<KT>(&sh, &d, reqs_small[item], cslot);
   }
 }
 

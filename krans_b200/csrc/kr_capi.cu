@@ -4,6 +4,7 @@
 #include <cmath>
 #include <cstring>
 #include <random>
+#include <vector>
 
 #include "kr_device.cuh"
 #include "kr_internal.h"
@@ -80,9 +81,11 @@ struct TeamFlat {
 
 template <class VT, class XT, class YT>
 __global__ void __launch_bounds__(256) spmv_kernel(int64_t rows, const int32_t *rp, const int32_t *ci,
-                                                   const VT *val, const XT *x, YT *y, int lanes) {
+                                                   const VT *val, const XT *x, YT *y, int lanes, int32_t ulen) {
   TeamFlat tm;
-  team_spmv(tm, rows, rp, ci, val, x, lanes, [&](int64_t i, typename AccOf<VT>::T s) { y[i] = (YT)s; });
+  team_spmv_x(
+      tm, rows, rp, ci, val, [&](int32_t c) { return x[c]; }, lanes, ulen,
+      [&](int64_t i, typename AccOf<VT>::T s) { y[i] = (YT)s; });
 }
 
 // two-stage deterministic reduction: partial per block, then one block sums
@@ -427,6 +430,23 @@ int krans_csr_create(krans_ctx *ctx, int64_t m, int64_t n, int64_t nnz, const in
   }
   A->lanes = pick_lanes(m, nnz);
   A->lanesT = pick_lanes(n, nnz);
+  // uniform row lengths (e.g. incidence and difference operators) let the
+  // SpMV skip the row pointers and use vector loads
+  {
+    const int64_t L = m > 0 ? (int64_t)(row_ptr[1] - row_ptr[0]) : 0;
+    bool uni = m > 0 && L > 0 && L <= 8;
+    for (int64_t i = 0; uni && i < m; i++)
+      uni = (int64_t)(row_ptr[i + 1] - row_ptr[i]) == L;
+    A->ulen = uni ? (int32_t)L : 0;
+    std::vector<int32_t> cc((size_t)n, 0);
+    for (int64_t k = 0; k < nnz; k++)
+      cc[(size_t)col_idx[k]]++;
+    const int32_t LT = n > 0 ? cc[0] : 0;
+    bool uniT = n > 0 && LT > 0 && LT <= 8;
+    for (int64_t j = 0; uniT && j < n; j++)
+      uniT = cc[(size_t)j] == LT;
+    A->ulenT = uniT ? LT : 0;
+  }
   *out = A;
   return KRANS_OK;
 }
@@ -620,10 +640,10 @@ int krans_spmv_ex(const krans_mat *A, int trans, int precision, const krans_vec 
   if (precision == KRANS_PREC_MIXED) {
     KR_CHECK_ARG(A->v32, "krans_spmv: matrix has no FP32 values (create with KRANS_CSR_FP32)");
     spmv_kernel<float, double, double><<<g, 256, 0, c->stream>>>(rows, rp, ci, trans ? A->vT32 : A->v32,
-                                                                 x->d, y->d, lanes);
+                                                                 x->d, y->d, lanes, trans ? A->ulenT : A->ulen);
   } else {
     spmv_kernel<double, double, double><<<g, 256, 0, c->stream>>>(rows, rp, ci, trans ? A->vT : A->v, x->d,
-                                                                  y->d, lanes);
+                                                                  y->d, lanes, trans ? A->ulenT : A->ulen);
   }
   KR_CUDA(cudaGetLastError());
   return KRANS_OK;

@@ -28,6 +28,7 @@ namespace kr {
 struct Counters {
   int64_t spmv = 0, spmvT = 0, cg_solves = 0, cg_maxit_hits = 0, steps = 0, restarts = 0;
   double bytes = 0.0;
+  uint64_t t_gk = 0, t_tiny = 0, t_cg = 0; // device time per phase (ns), leader's clock
 };
 
 template <class Team, class KT> struct CyclicSolver {
@@ -57,14 +58,14 @@ template <class Team, class KT> struct CyclicSolver {
 
   // y = F x (FP64)
   KR_DEV void mulF(const double *x, double *y) {
-    team_spmv(tm, d.F.rows, d.F.rp, d.F.ci, d.F.v64, x, d.F.lanes,
+    csr_mv(tm, d.F, d.F.v64, x,
               [&](int64_t i, double s) { y[i] = s; });
     count_F();
     c.bytes += spmv_bytes(d.F.rows, d.F.cols, d.F.nnz, 8, 8, 8);
     tm.sync();
   }
   KR_DEV void mulB(const double *x, double *y) {
-    team_spmv(tm, d.B.rows, d.B.rp, d.B.ci, d.B.v64, x, d.B.lanes,
+    csr_mv(tm, d.B, d.B.v64, x,
               [&](int64_t i, double s) { y[i] = s; });
     count_B();
     c.bytes += spmv_bytes(d.B.rows, d.B.cols, d.B.nnz, 8, 8, 8);
@@ -73,7 +74,7 @@ template <class Team, class KT> struct CyclicSolver {
   // ||F x|| with y = F x stored (fused norm)
   KR_DEV double mulF_norm(const double *x, double *y) {
     double s2 = 0.0;
-    team_spmv(tm, d.F.rows, d.F.rp, d.F.ci, d.F.v64, x, d.F.lanes, [&](int64_t i, double s) {
+    csr_mv(tm, d.F, d.F.v64, x, [&](int64_t i, double s) {
       y[i] = s;
       s2 += s * s;
     });
@@ -167,16 +168,29 @@ template <class Team, class KT> struct CyclicSolver {
     *rnorm_out = rnorm;
     if (rnorm <= tol)
       return 0;
+    // p = r at entry. Each iteration first forms p <- r + beta p; that
+    // update is folded into the gather of the first SpMV (t = F^T p) and into
+    // the epilogue of the second (which stores p), so CG needs no separate
+    // pass over p (fma(beta, p, r) in both places: the same values).
     int64_t k = 0;
+    double beta = 0.0;
     for (; k < maxit && tm.ok(); ++k) {
-      mulB(p, tn);
+      const double bq = beta;
+      team_spmv_x(
+          tm, d.B.rows, d.B.rp, d.B.ci, d.B.v64, [&](int32_t cc) { return r[cc] + bq * p[cc]; }, d.B.lanes,
+          d.B.ulen, [&](int64_t i, double s) { tn[i] = s; });
+      count_B();
+      c.bytes += spmv_bytes(d.B.rows, d.B.cols, d.B.nnz, 8, 8, 8) + 8.0 * m;
+      tm.sync();
       double pap = 0.0;
-      team_spmv(tm, d.F.rows, d.F.rp, d.F.ci, d.F.v64, tn, d.F.lanes, [&](int64_t i, double s) {
+      csr_mv(tm, d.F, d.F.v64, tn, [&](int64_t i, double s) {
+        const double pn = r[i] + bq * p[i];
+        p[i] = pn;
         Ap[i] = s;
-        pap += p[i] * s;
+        pap += pn * s;
       });
       count_F();
-      c.bytes += spmv_bytes(d.F.rows, d.F.cols, d.F.nnz, 8, 8, 8) + 8.0 * m;
+      c.bytes += spmv_bytes(d.F.rows, d.F.cols, d.F.nnz, 8, 8, 8) + 24.0 * m;
       pap = tm.sum1(pap);
       if (!isfinite(pap) || fabs(pap) <= bd_tol)
         break;
@@ -201,7 +215,7 @@ template <class Team, class KT> struct CyclicSolver {
             rzn += ri * ri;
           }
       });
-      rzn = tm.sum1(rzn);
+      rzn = tm.sum1(rzn); // its barrier also publishes r for the next gather
       c.bytes += 40.0 * m;
       if (!isfinite(rzn))
         break;
@@ -210,23 +224,8 @@ template <class Team, class KT> struct CyclicSolver {
         ++k;
         break;
       }
-      const double beta = rzn / fmax(1e-300, rz);
+      beta = rzn / fmax(1e-300, rz);
       rz = rzn;
-      team_for4(tm, m, [&](const int64_t *ix, int cnt) {
-        double pv[4], rv[4];
-#pragma unroll
-        for (int u = 0; u < 4; u++)
-          if (u < cnt) {
-            pv[u] = p[ix[u]];
-            rv[u] = r[ix[u]];
-          }
-#pragma unroll
-        for (int u = 0; u < 4; u++)
-          if (u < cnt)
-            p[ix[u]] = pv[u] * beta + rv[u];
-      });
-      c.bytes += 24.0 * m;
-      tm.sync();
     }
     *rnorm_out = rnorm;
     return k;
@@ -425,6 +424,7 @@ template <class Team, class KT> struct CyclicSolver {
     const int64_t k_target = d.k_target, ncv = d.ncv;
     bool converged = false;
 
+    const uint64_t t_run0 = globaltimer_ns();
     frob = fro_est();
     const double fmx = fmax(1.0, frob);
     const double accept = fmax(o.tol_abs, o.tol_rel * fmx);
@@ -459,6 +459,7 @@ template <class Team, class KT> struct CyclicSolver {
         c.bytes += (8.0 + 8.0 + sizeof(KT)) * n;
         tm.sync();
       }
+      const uint64_t t_gk0 = globaltimer_ns();
       int nY = 1, nX = 0, na = 0, nbeta = 0;
       int64_t local_steps = 0;
       double beta_last = 0.0, beta_prev = 0.0; // beta_prev: uniform register copy
@@ -470,10 +471,10 @@ template <class Team, class KT> struct CyclicSolver {
           const KT bp = (KT)(nbeta > 0 ? beta_prev : 0.0);
           const bool sub = nbeta > 0;
           if constexpr (sizeof(KT) == 8) {
-            team_spmv(tm, d.F.rows, d.F.rp, d.F.ci, d.F.v64, yj, d.F.lanes,
+            csr_mv(tm, d.F, d.F.v64, yj,
                       [&](int64_t i, double s) { wx[i] = sub ? (KT)(s - (double)bp * (double)xp[i]) : (KT)s; });
           } else {
-            team_spmv(tm, d.F.rows, d.F.rp, d.F.ci, d.F.v32, yj, d.F.lanes,
+            csr_mv(tm, d.F, d.F.v32, yj,
                       [&](int64_t i, float s) { wx[i] = sub ? (KT)(s - (float)bp * (float)xp[i]) : (KT)s; });
           }
           count_F();
@@ -487,10 +488,10 @@ template <class Team, class KT> struct CyclicSolver {
           const KT *yp = Y + (int64_t)(nY - 1) * ldn;
           const KT bp = (KT)beta_prev;
           if constexpr (sizeof(KT) == 8) {
-            team_spmv(tm, d.B.rows, d.B.rp, d.B.ci, d.B.v64, xj, d.B.lanes,
+            csr_mv(tm, d.B, d.B.v64, xj,
                       [&](int64_t i, double s) { wy[i] = (KT)(s - (double)bp * (double)yp[i]); });
           } else {
-            team_spmv(tm, d.B.rows, d.B.rp, d.B.ci, d.B.v32, xj, d.B.lanes,
+            csr_mv(tm, d.B, d.B.v32, xj,
                       [&](int64_t i, float s) { wy[i] = (KT)(s - (float)bp * (float)yp[i]); });
           }
           count_B();
@@ -533,12 +534,15 @@ template <class Team, class KT> struct CyclicSolver {
       }
       c.steps += local_steps;
       tm.publish(); // alpha/beta written by the leader
+      c.t_gk += globaltimer_ns() - t_gk0;
       const int l = na;
       if (l == 0 || !isfinite(beta_last) || !tm.ok())
         break;
 
       const bool split = (o.use_harmonic != 0) && o.target_tau == 0.0;
+      const uint64_t t_ti0 = globaltimer_ns();
       const int ncand = tiny_problem(l, beta_last, nY);
+      c.t_tiny += globaltimer_ns() - t_ti0;
       if (ncand < 0) {
         random(y0);
         gs2_basis(y0);
@@ -607,7 +611,9 @@ template <class Team, class KT> struct CyclicSolver {
         const int passes = o.projector_passes > 1 ? o.projector_passes : 1;
         for (int pass = 0; pass < passes && res > accept && tm.ok(); ++pass) {
           double rn;
+          const uint64_t t_cg0 = globaltimer_ns();
           cg_its = cg(tmv, wm, o.cg_maxit, o.cg_rel_tol, o.cg_breakdown_tol, &rn);
+          c.t_cg += globaltimer_ns() - t_cg0;
           c.cg_solves++;
           if (cg_its >= o.cg_maxit) {
             c.cg_maxit_hits++;
@@ -690,6 +696,11 @@ template <class Team, class KT> struct CyclicSolver {
       R->bytes = c.bytes;
       R->converged = converged ? 1 : 0;
       R->status = *(volatile int *)d.status;
+      const double tot = (double)(globaltimer_ns() - t_run0) * 1e-6;
+      R->phase_ms[0] = (double)c.t_gk * 1e-6;
+      R->phase_ms[1] = (double)c.t_tiny * 1e-6;
+      R->phase_ms[2] = (double)c.t_cg * 1e-6;
+      R->phase_ms[3] = tot - R->phase_ms[0] - R->phase_ms[1] - R->phase_ms[2];
     }
   }
 };

@@ -22,6 +22,9 @@
 #ifndef KR_RED_K
 #define KR_RED_K 8 // values per fused team reduction
 #endif
+#ifndef KR_SPMV_ROWS
+#define KR_SPMV_ROWS 4 // row groups each warp keeps in flight in team_spmv
+#endif
 
 namespace kr {
 
@@ -372,17 +375,113 @@ template <class Acc> struct AccOf;
 template <> struct AccOf<double> { using T = double; };
 template <> struct AccOf<float> { using T = float; };
 
-template <class Team, class VT, class XT, class Epi>
-KR_DEV void team_spmv(Team &tm, int64_t rows, const int32_t *__restrict__ rp,
-                      const int32_t *__restrict__ ci, const VT *__restrict__ val,
-                      const XT *__restrict__ x, int lanes, Epi epi) {
-  // Each warp walks R row groups at once: all row pointers, then all
-  // (column, value) pairs, then all x gathers are issued before the FMAs, so
-  // a thread keeps R independent loads in flight. Lane `sub` of a row sums
-  // the entries b+sub, b+sub+lanes, ... in order, then a fixed butterfly
-  // combines the lanes: the result does not depend on R or on the team.
+// Thread-per-row SpMV for matrices whose rows all hold exactly L entries
+// (L == lanes): no row pointers, vector loads of the (column, value) pairs.
+// The products are combined with the same tree as the lane butterfly of
+// team_spmv_x, so both paths give bit-identical results.
+template <int L, class Team, class VT, class GX, class Epi>
+KR_DEV void team_spmv_uniform(Team &tm, int64_t rows, const int32_t *__restrict__ ci,
+                              const VT *__restrict__ val, GX gx, Epi epi) {
   using Acc = typename AccOf<VT>::T;
-  constexpr int R = 4;
+  using XT = decltype(gx(0));
+  constexpr int R = KR_SPMV_ROWS;
+  const int64_t nt = tm.nthreads();
+  for (int64_t i0 = tm.tid(); i0 < rows; i0 += (int64_t)R * nt) {
+    int32_t c[R][L];
+    VT v[R][L];
+#pragma unroll
+    for (int u = 0; u < R; u++) {
+      const int64_t i = i0 + (int64_t)u * nt;
+      if (i < rows) {
+        if constexpr (L == 2) {
+          const int2 cc = __ldg(reinterpret_cast<const int2 *>(ci) + i);
+          c[u][0] = cc.x;
+          c[u][1] = cc.y;
+          if constexpr (sizeof(VT) == 8) {
+            const double2 vv = __ldg(reinterpret_cast<const double2 *>(val) + i);
+            v[u][0] = vv.x;
+            v[u][1] = vv.y;
+          } else {
+            const float2 vv = __ldg(reinterpret_cast<const float2 *>(val) + i);
+            v[u][0] = vv.x;
+            v[u][1] = vv.y;
+          }
+        } else if constexpr (L == 4) {
+          const int4 cc = __ldg(reinterpret_cast<const int4 *>(ci) + i);
+          c[u][0] = cc.x;
+          c[u][1] = cc.y;
+          c[u][2] = cc.z;
+          c[u][3] = cc.w;
+#pragma unroll
+          for (int j = 0; j < 4; j++)
+            v[u][j] = __ldg(val + i * 4 + j);
+        } else {
+#pragma unroll
+          for (int j = 0; j < L; j++) {
+            c[u][j] = __ldg(ci + i * L + j);
+            v[u][j] = __ldg(val + i * L + j);
+          }
+        }
+      } else {
+#pragma unroll
+        for (int j = 0; j < L; j++) {
+          c[u][j] = 0;
+          v[u][j] = VT(0);
+        }
+      }
+    }
+    XT xv[R][L];
+#pragma unroll
+    for (int u = 0; u < R; u++)
+#pragma unroll
+      for (int j = 0; j < L; j++)
+        xv[u][j] = (i0 + (int64_t)u * nt < rows) ? gx(c[u][j]) : XT(0);
+#pragma unroll
+    for (int u = 0; u < R; u++) {
+      const int64_t i = i0 + (int64_t)u * nt;
+      Acc p[L];
+#pragma unroll
+      for (int j = 0; j < L; j++)
+        p[j] = Acc(0) + (Acc)v[u][j] * (Acc)xv[u][j];
+#pragma unroll
+      for (int o = L / 2; o > 0; o /= 2)
+#pragma unroll
+        for (int j = 0; j < o; j++)
+          p[j] = p[j] + p[j + o];
+      if (i < rows)
+        epi(i, p[0]);
+    }
+  }
+}
+
+// CSR SpMV inside a team with a gather functor gx(col) for the input vector.
+// `lanes` threads per row (power of two <= 32), rows handed out in
+// warp-uniform blocks so the shuffles see full warps; each warp walks R row
+// groups at once (all row pointers, then all (column, value) pairs, then all
+// gathers are issued before the FMAs). Lane `sub` of a row sums the entries
+// b+sub, b+sub+lanes, ... in order, then a fixed butterfly combines the
+// lanes: the result does not depend on R or on the team. The epilogue gets
+// (row, sum) on the first lane of the row group.
+template <class Team, class VT, class GX, class Epi>
+KR_DEV void team_spmv_x(Team &tm, int64_t rows, const int32_t *__restrict__ rp, const int32_t *__restrict__ ci,
+                        const VT *__restrict__ val, GX gx, int lanes, int32_t ulen, Epi epi) {
+  if (ulen == lanes) {
+    if (ulen == 2) {
+      team_spmv_uniform<2>(tm, rows, ci, val, gx, epi);
+      return;
+    }
+    if (ulen == 4) {
+      team_spmv_uniform<4>(tm, rows, ci, val, gx, epi);
+      return;
+    }
+    if (ulen == 1) {
+      team_spmv_uniform<1>(tm, rows, ci, val, gx, epi);
+      return;
+    }
+  }
+  using Acc = typename AccOf<VT>::T;
+  using XT = decltype(gx(0));
+  constexpr int R = KR_SPMV_ROWS;
   const int lane = threadIdx.x & 31;
   const int sub = lane & (lanes - 1), grp = lane / lanes;
   const int rpw = 32 / lanes;
@@ -419,7 +518,7 @@ KR_DEV void team_spmv(Team &tm, int64_t rows, const int32_t *__restrict__ rp,
       XT xv[R];
 #pragma unroll
       for (int u = 0; u < R; u++)
-        xv[u] = ok[u] ? x[c[u]] : XT(0);
+        xv[u] = ok[u] ? gx(c[u]) : XT(0);
 #pragma unroll
       for (int u = 0; u < R; u++)
         if (ok[u])
@@ -436,6 +535,18 @@ KR_DEV void team_spmv(Team &tm, int64_t rows, const int32_t *__restrict__ rp,
         epi(i, s[u]);
     }
   }
+}
+
+template <class Team, class VT, class XT, class Epi>
+KR_DEV void team_spmv(Team &tm, int64_t rows, const int32_t *__restrict__ rp, const int32_t *__restrict__ ci,
+                      const VT *__restrict__ val, const XT *__restrict__ x, int lanes, Epi epi) {
+  team_spmv_x(tm, rows, rp, ci, val, [&](int32_t c) { return x[c]; }, lanes, 0, epi);
+}
+
+// y = V x over a CsrView (uses the uniform-row-length path when it applies)
+template <class Team, class VT, class XT, class Epi>
+KR_DEV void csr_mv(Team &tm, const CsrView &V, const VT *val, const XT *__restrict__ x, Epi epi) {
+  team_spmv_x(tm, V.rows, V.rp, V.ci, val, [&](int32_t c) { return x[c]; }, V.lanes, V.ulen, epi);
 }
 
 // Algorithmic HBM bytes of one CSR SpMV (rows r, cols c, nnz z, value width

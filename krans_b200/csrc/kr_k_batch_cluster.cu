@@ -38,12 +38,16 @@ int cyclic_batch_cluster_max(bool mixed, int csize, int sms) {
 }
 
 cudaError_t launch_cyclic_batch_cluster(bool mixed, int nclusters, int csize, cudaStream_t s,
-                                        const CyclicRequestDev *reqs, int count, int *queue, char *ws, size_t stride) {
+                                        const CyclicRequestDev *reqs_large, int n_large, int *queue_large,
+                                        char *ws_large, size_t stride_large, const CyclicRequestDev *reqs_small,
+                                        int n_small, int *queue_small, char *ws_small, size_t stride_small) {
   cudaLaunchAttribute at[1];
   cudaLaunchConfig_t cfg = cl_config(nclusters, csize, s, at);
   if (mixed)
-    return cudaLaunchKernelEx(&cfg, cyclic_batch_cluster_kernel<float>, reqs, count, queue, ws, stride);
-  return cudaLaunchKernelEx(&cfg, cyclic_batch_cluster_kernel<double>, reqs, count, queue, ws, stride);
+    return cudaLaunchKernelEx(&cfg, cyclic_batch_cluster_kernel<float>, reqs_large, n_large, queue_large, ws_large,
+                              stride_large, reqs_small, n_small, queue_small, ws_small, stride_small);
+  return cudaLaunchKernelEx(&cfg, cyclic_batch_cluster_kernel<double>, reqs_large, n_large, queue_large, ws_large,
+                            stride_large, reqs_small, n_small, queue_small, ws_small, stride_small);
 }
 
 } // namespace kr

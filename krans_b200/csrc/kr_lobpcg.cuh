@@ -36,20 +36,20 @@ template <class Team> struct LobpcgSolver {
 
   // ---- primitives ---------------------------------------------------------
   KR_DEV void mulA(const double *x, double *y) {
-    team_spmv(tm, d.F.rows, d.F.rp, d.F.ci, d.F.v64, x, d.F.lanes, [&](int64_t i, double s) { y[i] = s; });
+    csr_mv(tm, d.F, d.F.v64, x, [&](int64_t i, double s) { y[i] = s; });
     c.spmv++;
     c.bytes += spmv_bytes(m, n, d.F.nnz, 8, 8, 8);
     tm.sync();
   }
   KR_DEV void mulAT(const double *x, double *y) {
-    team_spmv(tm, d.B.rows, d.B.rp, d.B.ci, d.B.v64, x, d.B.lanes, [&](int64_t i, double s) { y[i] = s; });
+    csr_mv(tm, d.B, d.B.v64, x, [&](int64_t i, double s) { y[i] = s; });
     c.spmvT++;
     c.bytes += spmv_bytes(n, m, d.B.nnz, 8, 8, 8);
     tm.sync();
   }
   KR_DEV double normA(const double *x, double *y) { // ||A x||, y = A x
     double s2 = 0.0;
-    team_spmv(tm, d.F.rows, d.F.rp, d.F.ci, d.F.v64, x, d.F.lanes, [&](int64_t i, double s) {
+    csr_mv(tm, d.F, d.F.v64, x, [&](int64_t i, double s) {
       y[i] = s;
       s2 += s * s;
     });

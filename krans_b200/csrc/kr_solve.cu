@@ -19,9 +19,9 @@ static size_t cyclic_layout(const CyclicPlan &p, char *base, CyclicDesc *d) { re
 static CsrView view_of(const krans_mat *A, bool trans) {
   CsrView v;
   if (!trans) {
-    v = CsrView{A->m, A->n, A->nnz, A->rp, A->ci, A->v, A->v32, A->lanes};
+    v = CsrView{A->m, A->n, A->nnz, A->rp, A->ci, A->v, A->v32, A->lanes, A->ulen};
   } else {
-    v = CsrView{A->n, A->m, A->nnz, A->rpT, A->ciT, A->vT, A->vT32, A->lanesT};
+    v = CsrView{A->n, A->m, A->nnz, A->rpT, A->ciT, A->vT, A->vT32, A->lanesT, A->ulenT};
   }
   return v;
 }
@@ -238,6 +238,8 @@ extern "C" int krans_solve_cyclic(krans_ctx *ctx, const krans_mat *A, krans_rng 
     result->spmvT = ro.r.spmvT;
     result->algo_bytes = ro.r.bytes;
     result->device_ms = ro.ms;
+    for (int q = 0; q < 4; q++)
+      result->phase_ms[q] = ro.r.phase_ms[q];
   }
   for (size_t i = 0; i < right.size(); i++)
     right_out[i] = right[i];

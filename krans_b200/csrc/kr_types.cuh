@@ -39,7 +39,8 @@ struct CsrView {
   const int32_t *rp, *ci;
   const double *v64;
   const float *v32;
-  int lanes; // threads per row in the SpMV
+  int lanes;    // threads per row in the SpMV
+  int32_t ulen; // every row has exactly ulen entries (rp[i] = i*ulen), 0 if not
 };
 
 struct CyclicDevResult {
@@ -49,6 +50,7 @@ struct CyclicDevResult {
   int32_t converged;
   int32_t status;
   uint64_t t_begin, t_end; // device globaltimer (ns) when the request started / finished
+  double phase_ms[4];      // device time in: Golub-Kahan + reorth, tiny SVD, CG polish, the rest
 };
 
 struct CyclicDesc {
@@ -206,7 +208,9 @@ cudaError_t launch_cyclic_batch_cta(bool mixed, int grid, cudaStream_t s, const 
                                     int *queue, char *ws, size_t stride);
 int cyclic_batch_cluster_max(bool mixed, int csize, int sms);
 cudaError_t launch_cyclic_batch_cluster(bool mixed, int nclusters, int csize, cudaStream_t s,
-                                        const CyclicRequestDev *reqs, int count, int *queue, char *ws, size_t stride);
+                                        const CyclicRequestDev *reqs_large, int n_large, int *queue_large,
+                                        char *ws_large, size_t stride_large, const CyclicRequestDev *reqs_small,
+                                        int n_small, int *queue_small, char *ws_small, size_t stride_small);
 int lobpcg_grid_blocks(krans_ctx *ctx, int threads);
 cudaError_t launch_lobpcg(bool grid, const LobpcgDesc &d, const LobpcgDesc *d_dev, int blocks, int threads,
                           cudaStream_t s);
