@@ -50,6 +50,7 @@ struct CyclicLanczosOptions {
   // B200 engine knobs (no reference counterpart)
   int precision = KRANS_PREC_FP64; // KRANS_PREC_MIXED: FP32 SpMV/Lanczos, FP64 reorth/SVD/polish
   int team = KRANS_TEAM_AUTO;
+  int polish_block = 0; // 1: project up to 8 candidates per restart with one block CG
 };
 
 struct CyclicLanczosResult {
@@ -96,6 +97,7 @@ inline CyclicLanczosResult find_nullspace_cyclic_lanczos_ex(const MatrixInterfac
   o.verbose = opt.verbose;
   o.precision = opt.precision;
   o.team = opt.team;
+  o.polish_block = opt.polish_block;
   const krans_vec *y0 = nullptr;
   if (!opt.initial_right_space.empty() && opt.initial_right_space.front()) {
     const auto *c = dynamic_cast<const cuda::CudaVectorAdapter *>(opt.initial_right_space.front().get());

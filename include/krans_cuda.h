@@ -165,6 +165,9 @@ typedef struct krans_cyclic_opts {
   /* B200 engine knobs (no reference counterpart) */
   int32_t precision;         /* KRANS_PREC_FP64 */
   int32_t team;              /* KRANS_TEAM_AUTO */
+  int32_t polish_block;      /* 0: polish candidates one by one (the reference's order);
+                                1: project up to 8 candidates of a restart with one block CG
+                                (matrix read once per iteration for all of them) */
 } krans_cyclic_opts;
 
 typedef struct krans_cyclic_result {

@@ -46,7 +46,8 @@ class CyclicOpts(C.Structure):
                 ("projector_passes", C.c_int32), ("grad_max_iters", C.c_int32),
                 ("frob_samples", C.c_int32), ("prescreen_factor", C.c_double),
                 ("stagnation_restarts", C.c_int64), ("return_left_space", C.c_int32),
-                ("verbose", C.c_int32), ("precision", C.c_int32), ("team", C.c_int32)]
+                ("verbose", C.c_int32), ("precision", C.c_int32), ("team", C.c_int32),
+                ("polish_block", C.c_int32)]
 
 
 class CyclicResultC(C.Structure):

@@ -302,6 +302,7 @@ class CyclicLanczosOptions:
     # engine knobs (no reference counterpart)
     precision: Precision = Precision.FP64
     team: int = K.KRANS_TEAM_AUTO
+    polish_block: int = 0  # 1: block CG polish of up to 8 candidates at once
 
     def to_c(self) -> K.CyclicOpts:
         o = K.CyclicOpts()

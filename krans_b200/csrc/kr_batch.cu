@@ -123,6 +123,7 @@ struct BatchLaunch {
       q.plan.ksz = precision == KRANS_PREC_MIXED ? 4 : 8;
       q.plan.grid_blocks = 1;
       q.plan.own_basis = 0;
+      q.plan.block_polish = r.opts.polish_block ? 1 : 0;
       q.basis = r.basis_out;
       if (!trivial) {
         if (pos < n_large)

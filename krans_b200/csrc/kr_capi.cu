@@ -749,6 +749,7 @@ int krans_cyclic_opts_init(krans_cyclic_opts *o) {
   o->verbose = 0;
   o->precision = KRANS_PREC_FP64;
   o->team = KRANS_TEAM_AUTO;
+  o->polish_block = 0;
   return KRANS_OK;
 }
 

@@ -231,6 +231,152 @@ template <class Team, class KT> struct CyclicSolver {
     return k;
   }
 
+  // Per-column totals of a value each thread holds for its own column
+  // (column = thread index mod KR_NBP); every thread receives all KR_NBP totals.
+  KR_DEV void col_sums(double x, double (&t)[KR_NBP]) {
+    const int col = (int)(threadIdx.x & (KR_NBP - 1));
+#pragma unroll
+    for (int q = 0; q < KR_NBP; q++)
+      t[q] = q == col ? x : 0.0;
+    tm.template sum<KR_NBP>(t);
+  }
+  KR_DEV static double pick(const double (&t)[KR_NBP], int col) {
+    double r = 0.0;
+#pragma unroll
+    for (int q = 0; q < KR_NBP; q++)
+      if (q == col)
+        r = t[q];
+    return r;
+  }
+
+  // Block CG on (F F^T) W = H for the first nc <= KR_NBP interleaved columns
+  // of d.Hb (solutions in d.Wb). Every column follows the rules of cg()
+  // above on its own: same start, breakdown, finiteness and tolerance tests,
+  // and a column that stops is never touched again; one iteration reads the
+  // matrix once for all columns still running. The iteration count of column
+  // q is left in tm.sh->ibuf[q].
+  __device__ __noinline__ void cg_block(int nc, int64_t maxit, double rel_tol, double bd_tol) {
+    const int col = (int)(threadIdx.x & (KR_NBP - 1));
+    double *R = d.Rk, *P = d.Pk, *AP = d.Ak, *W = d.Wb, *T = d.Tk;
+    const double *H = d.Hb;
+    const int64_t mb = m * KR_NBP;
+    double t[KR_NBP];
+    double rr = 0.0;
+    team_for(tm, mb, [&](int64_t e) {
+      const double h = col < nc ? H[e] : 0.0;
+      W[e] = 0.0;
+      R[e] = h;
+      P[e] = h;
+      rr += h * h;
+    });
+    col_sums(rr, t);
+    c.bytes += 32.0 * m * nc;
+    unsigned act = 0;
+    double tol[KR_NBP];
+    int64_t its[KR_NBP];
+#pragma unroll
+    for (int q = 0; q < KR_NBP; q++) {
+      its[q] = 0;
+      const double rn = sqrt(t[q] > 0.0 ? t[q] : 0.0);
+      tol[q] = fmax(rel_tol * rn, 1e-30);
+      if (q < nc && rn > 0.0 && isfinite(rn) && rn > tol[q])
+        act |= 1u << q;
+    }
+    double rz = pick(t, col), beta = 0.0; // this thread's column
+    int64_t k = 0;
+    for (; k < maxit && act && tm.ok(); ++k) {
+      const int na = __popc(act);
+      const bool mine = (act >> col) & 1u;
+      const double bq = beta;
+      // T = F^T (R + beta P): the direction update folded into the gather
+      team_spmv_block(
+          tm, d.B.rows, d.B.rp, d.B.ci, d.B.v64, d.B.ulen, mine,
+          [&](int32_t cc) {
+            const int64_t e = (int64_t)cc * KR_NBP + col;
+            return R[e] + bq * P[e];
+          },
+          [&](int64_t i, double s) { T[i * KR_NBP + col] = s; });
+      c.spmvT += d.trans_run ? 0 : na;
+      c.spmv += d.trans_run ? na : 0;
+      c.bytes += spmv_bytes(d.B.rows, d.B.cols, d.B.nnz, 8, 16 * na, 8 * na);
+      tm.sync();
+      double pap = 0.0;
+      team_spmv_block(
+          tm, d.F.rows, d.F.rp, d.F.ci, d.F.v64, d.F.ulen, mine, [&](int32_t cc) { return T[(int64_t)cc * KR_NBP + col]; },
+          [&](int64_t i, double s) {
+            const int64_t e = i * KR_NBP + col;
+            const double pn = R[e] + bq * P[e];
+            P[e] = pn;
+            AP[e] = s;
+            pap += pn * s;
+          });
+      c.spmv += d.trans_run ? 0 : na;
+      c.spmvT += d.trans_run ? na : 0;
+      c.bytes += spmv_bytes(d.F.rows, d.F.cols, d.F.nnz, 8, 8 * na, 8 * na) + 24.0 * m * na;
+      col_sums(pap, t);
+#pragma unroll
+      for (int q = 0; q < KR_NBP; q++)
+        if (((act >> q) & 1u) && (!isfinite(t[q]) || fabs(t[q]) <= bd_tol)) {
+          its[q] = k;
+          act &= ~(1u << q);
+        }
+      const bool upd = (act >> col) & 1u;
+      const double alpha = upd ? rz / pick(t, col) : 0.0;
+      double rzn = 0.0;
+      team_for4(tm, mb, [&](const int64_t *ix, int cnt) {
+        if (!upd)
+          return;
+        double pv[4], wv[4], rv[4], av[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+          if (u < cnt) {
+            pv[u] = P[ix[u]];
+            wv[u] = W[ix[u]];
+            rv[u] = R[ix[u]];
+            av[u] = AP[ix[u]];
+          }
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+          if (u < cnt) {
+            W[ix[u]] = wv[u] + alpha * pv[u];
+            const double ri = rv[u] - alpha * av[u];
+            R[ix[u]] = ri;
+            rzn += ri * ri;
+          }
+      });
+      col_sums(rzn, t); // its barrier also publishes R for the next gather
+      c.bytes += 40.0 * m * na;
+#pragma unroll
+      for (int q = 0; q < KR_NBP; q++) {
+        if (!((act >> q) & 1u))
+          continue;
+        if (!isfinite(t[q])) {
+          its[q] = k;
+          act &= ~(1u << q);
+        } else if (sqrt(t[q] > 0.0 ? t[q] : 0.0) <= tol[q]) {
+          its[q] = k + 1;
+          act &= ~(1u << q);
+        }
+      }
+      if ((act >> col) & 1u) {
+        const double rzq = pick(t, col);
+        beta = rzq / fmax(1e-300, rz);
+        rz = rzq;
+      }
+    }
+    // columns still running ran out of iterations
+#pragma unroll
+    for (int q = 0; q < KR_NBP; q++)
+      if ((act >> q) & 1u)
+        its[q] = k;
+    if (threadIdx.x == 0) {
+#pragma unroll
+      for (int q = 0; q < KR_NBP; q++)
+        tm.sh->ibuf[q] = (int)its[q];
+    }
+    __syncthreads();
+  }
+
   // try_project_random_to_nullspace (CyclicLanczosSolver.cpp:140-214)
   __device__ __noinline__ bool try_project_random(double accept) {
     double *v = d.v, *tmv = d.tmv, *wm = d.wm, *tn = d.tn;
@@ -417,6 +563,196 @@ template <class Team, class KT> struct CyclicSolver {
     return *(volatile double *)&d.Vt[(size_t)jb * l + 2 * t];
   }
 
+  // candidate v = sum_q coef_q Y[q] (CyclicLanczosSolver.cpp:496-503)
+  KR_DEV void form_candidate(const KT *Y, bool split, int l, int jb, int ny_used, double *v) {
+    if (threadIdx.x < (unsigned)ny_used)
+      tm.sh->h[threadIdx.x] = coef(split, l, jb, threadIdx.x);
+    __syncthreads();
+    const int64_t ldn = d.ldn;
+    team_for4(tm, n, [&](const int64_t *ix, int cnt) {
+      double acc[4] = {0.0, 0.0, 0.0, 0.0};
+      for (int q = 0; q < ny_used; q++) {
+        const double hq = tm.sh->h[q];
+        const KT *yq = Y + (int64_t)q * ldn;
+        double yv[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+          yv[u] = u < cnt ? (double)yq[ix[u]] : 0.0;
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+          acc[u] += hq * yv[u];
+      }
+#pragma unroll
+      for (int u = 0; u < 4; u++)
+        if (u < cnt)
+          v[ix[u]] = acc[u];
+    });
+    c.bytes += (double)(ny_used * sizeof(KT) + 8) * n;
+    tm.sync();
+  }
+
+  struct CandState {
+    double best_res;
+    bool have_best, accepted_this, polish_stalled, converged;
+  };
+
+  // Candidate phase with the block polish: candidates are taken in the same
+  // order and screened by the same rules as the one-by-one loop of run(), but
+  // up to KR_NBP of those that need the projector are collected first and
+  // polished by one block CG. Each is then finished in order against the
+  // basis as it stands at that point (Gram-Schmidt, residual, acceptance), so
+  // an accepted vector is always orthogonal to the earlier ones. A candidate
+  // that already meets the tolerance is accepted when it is formed.
+  __device__ __noinline__ void candidates_block(const KT *Y, bool split, int l, int ncand, int64_t test_cap,
+                                                int ny_used, double prescreen, double accept, CandState &st) {
+    const krans_cyclic_opts &o = d.o;
+    const int64_t ldn = d.ldn;
+    double *Hb = d.Hb, *Tk = d.Tk;
+    double mres[KR_NBP];
+    int t = 0;
+    int64_t tested = 0;
+    while (t < ncand && tested < test_cap && tm.ok() && !st.converged) {
+      int g = 0;
+      while (g < KR_NBP && t < ncand && tested < test_cap && tm.ok()) {
+        const int jb = *(volatile int32_t *)&d.ord[t++];
+        double ce2 = 0.0;
+        for (int q = 0; q < ny_used; q++) {
+          const double cq = coef(split, l, jb, q);
+          ce2 += cq * cq;
+        }
+        if (!(ce2 >= 1e-20))
+          continue;
+        double *vg = d.Vc + (int64_t)g * ldn;
+        form_candidate(Y, split, l, jb, ny_used, vg);
+        gs2_basis(vg);
+        const double nv = nrm2(n, vg);
+        if (!isfinite(nv) || nv < 1e-8)
+          continue;
+        scale(n, 1.0 / nv, vg);
+        ++tested;
+        // residual, with F v stored as column g of the block right-hand side
+        double s2 = 0.0;
+        csr_mv(tm, d.F, d.F.v64, vg, [&](int64_t i, double s) {
+          Hb[i * KR_NBP + g] = s;
+          s2 += s * s;
+        });
+        count_F();
+        c.bytes += spmv_bytes(d.F.rows, d.F.cols, d.F.nnz, 8, 8, 8);
+        const double res = sqrt(tm.sum1(s2));
+        if (!isfinite(res))
+          continue;
+        if (res <= accept) {
+          copy(n, vg, d.basis + nb * d.ldb);
+          nb++;
+          st.accepted_this = true;
+          if (nb >= d.k_target) {
+            st.converged = true;
+            break;
+          }
+          continue;
+        }
+        if (res > prescreen || st.polish_stalled) {
+          if (res < st.best_res) {
+            st.best_res = res;
+            copy(n, vg, d.best_v);
+            st.have_best = true;
+          }
+          continue;
+        }
+        mres[g] = res;
+        g++;
+      }
+      if (st.converged || g == 0)
+        break;
+      const uint64_t t_cg0 = globaltimer_ns();
+      cg_block(g, o.cg_maxit, o.cg_rel_tol, o.cg_breakdown_tol);
+      c.t_cg += globaltimer_ns() - t_cg0;
+      // Tk = F^T W for all members at once
+      {
+        const int col = (int)(threadIdx.x & (KR_NBP - 1));
+        const double *W = d.Wb;
+        team_spmv_block(
+            tm, d.B.rows, d.B.rp, d.B.ci, d.B.v64, d.B.ulen, col < g, [&](int32_t cc) { return W[(int64_t)cc * KR_NBP + col]; },
+            [&](int64_t i, double s) { Tk[i * KR_NBP + col] = s; });
+        c.spmvT += d.trans_run ? 0 : g;
+        c.spmv += d.trans_run ? g : 0;
+        c.bytes += spmv_bytes(d.B.rows, d.B.cols, d.B.nnz, 8, 8 * g, 8 * g);
+        tm.sync();
+      }
+      int its[KR_NBP];
+#pragma unroll
+      for (int q = 0; q < KR_NBP; q++)
+        its[q] = tm.sh->ibuf[q];
+      __syncthreads();
+      const int passes = o.projector_passes > 1 ? o.projector_passes : 1;
+      for (int q = 0; q < g && tm.ok(); q++) {
+        double *v = d.Vc + (int64_t)q * ldn, *vp = d.vp, *tmv = d.tmv, *wm = d.wm;
+        double res = mres[q];
+        bool hit_maxit = false;
+        int its_q = 0;
+#pragma unroll
+        for (int u = 0; u < KR_NBP; u++)
+          if (u == q)
+            its_q = its[u];
+        c.cg_solves++;
+        if (its_q >= o.cg_maxit) {
+          c.cg_maxit_hits++;
+          hit_maxit = true;
+        }
+        for (int pass = 0; pass < passes && res > accept && tm.ok(); ++pass) {
+          if (pass == 0) {
+            team_for(tm, n, [&](int64_t i) { vp[i] = v[i] - Tk[i * KR_NBP + q]; });
+          } else {
+            double rn;
+            const uint64_t t_cg1 = globaltimer_ns();
+            const int64_t cg_its = cg(tmv, wm, o.cg_maxit, o.cg_rel_tol, o.cg_breakdown_tol, &rn);
+            c.t_cg += globaltimer_ns() - t_cg1;
+            c.cg_solves++;
+            if (cg_its >= o.cg_maxit) {
+              c.cg_maxit_hits++;
+              hit_maxit = true;
+            }
+            mulB(wm, d.tn);
+            team_for(tm, n, [&](int64_t i) { vp[i] = v[i] - d.tn[i]; });
+          }
+          c.bytes += 24.0 * n;
+          tm.sync();
+          gs2_basis(vp);
+          const double np = nrm2(n, vp);
+          if (!isfinite(np) || np < 1e-14)
+            break;
+          scale(n, 1.0 / np, vp);
+          const double res_p = mulF_norm(vp, wm);
+          if (!(res_p < res))
+            break;
+          double *t1 = v;
+          v = vp;
+          vp = t1;
+          res = res_p;
+          t1 = tmv;
+          tmv = wm;
+          wm = t1;
+        }
+        if (res <= accept) {
+          copy(n, v, d.basis + nb * d.ldb);
+          nb++;
+          st.accepted_this = true;
+          if (nb >= d.k_target) {
+            st.converged = true;
+            break;
+          }
+        } else {
+          st.polish_stalled = st.polish_stalled || hit_maxit;
+          if (res < st.best_res) {
+            st.best_res = res;
+            copy(n, v, d.best_v);
+            st.have_best = true;
+          }
+        }
+      }
+    }
+  }
+
   __device__ __noinline__ void run() {
     const krans_cyclic_opts &o = d.o;
     KT *Y = (KT *)d.Y, *X = (KT *)d.X, *wx = (KT *)d.wx, *wy = (KT *)d.wy;
@@ -556,7 +892,16 @@ template <class Team, class KT> struct CyclicSolver {
       bool have_best = false, accepted_this = false, polish_stalled = false;
       int64_t tested = 0;
       const int ny_used = split ? ncand : (l + 1) / 2;
-      for (int t = 0; t < ncand && tested < test_cap && tm.ok(); ++t) {
+      if (d.Vc) {
+        CandState st{best_res, have_best, accepted_this, polish_stalled, converged};
+        candidates_block(Y, split, l, ncand, test_cap, ny_used, prescreen, accept, st);
+        best_res = st.best_res;
+        have_best = st.have_best;
+        accepted_this = st.accepted_this;
+        converged = st.converged;
+        tested = test_cap; // the one-by-one loop below is skipped
+      }
+      for (int t = 0; t < ncand && tested < test_cap && tm.ok() && !d.Vc; ++t) {
         const int jb = *(volatile int32_t *)&d.ord[t];
         double ce2 = 0.0;
         for (int q = 0; q < ny_used; q++) {
@@ -565,30 +910,7 @@ template <class Team, class KT> struct CyclicSolver {
         }
         if (!(ce2 >= 1e-20))
           continue;
-        // candidate v = sum_q coef_q Y[q]
-        if (threadIdx.x < (unsigned)ny_used)
-          tm.sh->h[threadIdx.x] = coef(split, l, jb, threadIdx.x);
-        __syncthreads();
-        team_for4(tm, n, [&](const int64_t *ix, int cnt) {
-          double acc[4] = {0.0, 0.0, 0.0, 0.0};
-          for (int q = 0; q < ny_used; q++) {
-            const double hq = tm.sh->h[q];
-            const KT *yq = Y + (int64_t)q * ldn;
-            double yv[4];
-#pragma unroll
-            for (int u = 0; u < 4; u++)
-              yv[u] = u < cnt ? (double)yq[ix[u]] : 0.0;
-#pragma unroll
-            for (int u = 0; u < 4; u++)
-              acc[u] += hq * yv[u];
-          }
-#pragma unroll
-          for (int u = 0; u < 4; u++)
-            if (u < cnt)
-              v[ix[u]] = acc[u];
-        });
-        c.bytes += (double)(ny_used * sizeof(KT) + 8) * n;
-        tm.sync();
+        form_candidate(Y, split, l, jb, ny_used, v);
         gs2_basis(v);
         const double nv = nrm2(n, v);
         if (!isfinite(nv) || nv < 1e-8)

@@ -549,6 +549,117 @@ KR_DEV void csr_mv(Team &tm, const CsrView &V, const VT *val, const XT *__restri
   team_spmv_x(tm, V.rows, V.rp, V.ci, val, [&](int32_t c) { return x[c]; }, V.lanes, V.ulen, epi);
 }
 
+// CSR SpMV over KR_NBP right-hand sides stored interleaved (element (i, j) at
+// i * KR_NBP + j). Eight consecutive threads share a row and thread j of the
+// group owns column j (the team size is a multiple of KR_NBP, so a thread's
+// column never changes): the (column, value) loads are broadcast inside the
+// group and the gather reads 64 contiguous bytes per entry. Each thread sums
+// its column over the row's entries in storage order (the same order in both
+// variants below); threads whose column is not `active` skip the row. Every
+// thread keeps R rows in flight so the gathers of several rows overlap.
+template <int L, int R, class Team, class GX, class Epi>
+KR_DEV void team_spmv_block_uniform(Team &tm, int64_t rows, const int32_t *__restrict__ ci,
+                                    const double *__restrict__ val, GX gx, Epi epi) {
+  const int64_t ng = tm.nthreads() / KR_NBP;
+  for (int64_t i0 = tm.tid() / KR_NBP; i0 < rows; i0 += (int64_t)R * ng) {
+    int32_t c[R][L];
+    double v[R][L];
+#pragma unroll
+    for (int u = 0; u < R; u++) {
+      const int64_t i = i0 + (int64_t)u * ng;
+#pragma unroll
+      for (int j = 0; j < L; j++) {
+        c[u][j] = i < rows ? __ldg(ci + i * L + j) : 0;
+        v[u][j] = i < rows ? __ldg(val + i * L + j) : 0.0;
+      }
+    }
+    double xv[R][L];
+#pragma unroll
+    for (int u = 0; u < R; u++)
+#pragma unroll
+      for (int j = 0; j < L; j++)
+        xv[u][j] = i0 + (int64_t)u * ng < rows ? gx(c[u][j]) : 0.0;
+#pragma unroll
+    for (int u = 0; u < R; u++) {
+      const int64_t i = i0 + (int64_t)u * ng;
+      double s = 0.0;
+#pragma unroll
+      for (int j = 0; j < L; j++)
+        s += v[u][j] * xv[u][j];
+      if (i < rows)
+        epi(i, s);
+    }
+  }
+}
+
+template <class Team, class GX, class Epi>
+KR_DEV void team_spmv_block(Team &tm, int64_t rows, const int32_t *__restrict__ rp,
+                            const int32_t *__restrict__ ci, const double *__restrict__ val, int32_t ulen,
+                            bool active, GX gx, Epi epi) {
+  if (!active)
+    return; // no barrier inside: threads of inactive columns simply skip
+  if (ulen == 2) {
+    team_spmv_block_uniform<2, 4>(tm, rows, ci, val, gx, epi);
+    return;
+  }
+  if (ulen == 1) {
+    team_spmv_block_uniform<1, 8>(tm, rows, ci, val, gx, epi);
+    return;
+  }
+  if (ulen == 4) {
+    team_spmv_block_uniform<4, 2>(tm, rows, ci, val, gx, epi);
+    return;
+  }
+  constexpr int R = 4;
+  const int64_t ng = tm.nthreads() / KR_NBP;
+  for (int64_t i0 = tm.tid() / KR_NBP; i0 < rows; i0 += (int64_t)R * ng) {
+    int32_t b[R], e[R];
+#pragma unroll
+    for (int u = 0; u < R; u++) {
+      const int64_t i = i0 + (int64_t)u * ng;
+      b[u] = 0;
+      e[u] = 0;
+      if (i < rows) {
+        b[u] = __ldg(rp + i);
+        e[u] = __ldg(rp + i + 1);
+      }
+    }
+    double s[R];
+#pragma unroll
+    for (int u = 0; u < R; u++)
+      s[u] = 0.0;
+    for (int32_t j = 0;; ++j) {
+      int32_t c[R];
+      double v[R];
+      bool ok[R], more = false;
+#pragma unroll
+      for (int u = 0; u < R; u++) {
+        const int32_t k = b[u] + j;
+        ok[u] = k < e[u];
+        more |= (k + 1) < e[u];
+        c[u] = ok[u] ? __ldg(ci + k) : 0;
+        v[u] = ok[u] ? __ldg(val + k) : 0.0;
+      }
+      double xv[R];
+#pragma unroll
+      for (int u = 0; u < R; u++)
+        xv[u] = ok[u] ? gx(c[u]) : 0.0;
+#pragma unroll
+      for (int u = 0; u < R; u++)
+        if (ok[u])
+          s[u] += v[u] * xv[u];
+      if (!more)
+        break;
+    }
+#pragma unroll
+    for (int u = 0; u < R; u++) {
+      const int64_t i = i0 + (int64_t)u * ng;
+      if (i < rows)
+        epi(i, s[u]);
+    }
+  }
+}
+
 // Algorithmic HBM bytes of one CSR SpMV (rows r, cols c, nnz z, value width
 // w, x width wx, y width wy): row pointers, columns+values, x once, y once.
 __host__ __device__ inline double spmv_bytes(int64_t r, int64_t c, int64_t z, int w, int wx, int wy) {

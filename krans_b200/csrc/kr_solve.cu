@@ -82,6 +82,7 @@ static int run_cyclic(krans_ctx *ctx, const krans_mat *A, bool trans, krans_rng 
   p.ksz = mixed ? 4 : 8;
   p.grid_blocks = grid ? cyclic_grid_blocks(ctx, mixed, threads) : 1;
   p.own_basis = grid ? 1 : 0;
+  p.block_polish = o.polish_block ? 1 : 0;
   // one allocation: solver workspace, basis, request record and counters
   char *slot = nullptr;
   double *basis = nullptr, *d_mr = nullptr;
@@ -268,6 +269,7 @@ extern "C" int krans_solve_cyclic(krans_ctx *ctx, const krans_mat *A, krans_rng 
     lo.rank_known = o.rank_known;
     lo.precision = o.precision;
     lo.team = o.team;
+    lo.polish_block = o.polish_block;
     if (o.rank_known >= 0) {
       const int left_nullity = (int)A->m - o.rank_known;
       lo.nullity_known = std::max(0, std::min(left_nullity, (int)o.k));

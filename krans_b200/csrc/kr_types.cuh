@@ -12,6 +12,7 @@
 #ifndef KR_RED_K
 #define KR_RED_K 8 // values per fused team reduction
 #endif
+#define KR_NBP 8 // right-hand sides of the block CG polish (one fused reduction)
 
 namespace kr {
 
@@ -63,6 +64,8 @@ struct CyclicDesc {
   double *basis;               // k_target x ldn (output, row i = vector i)
   void *Y, *X, *wx, *wy;       // KT storage
   double *y0, *v, *vp, *best_v, *tn; // n-vectors
+  double *Vc;                        // KR_NBP candidate n-vectors (block polish)
+  double *Hb, *Wb, *Rk, *Pk, *Ak, *Tk; // interleaved CG blocks: m x KR_NBP (Tk: n x KR_NBP)
   double *tmv, *wm, *r, *p, *Ap;     // m-vectors
   double *alpha, *beta;              // ncv + 2
   double *Tb, *Vt, *sv;              // tiny problem
@@ -84,6 +87,7 @@ struct CyclicPlan {
   int32_t ksz;         // bytes of the Krylov storage type
   int32_t grid_blocks; // blocks of a grid team (reduction partials)
   int32_t own_basis;   // basis lives in the workspace (else in the request)
+  int32_t block_polish; // workspace for the block CG polish (KR_NBP candidates at once)
 };
 
 __host__ __device__ inline int64_t kr_round_up(int64_t x, int64_t a) { return (x + a - 1) / a * a; }
@@ -121,6 +125,16 @@ __host__ __device__ inline size_t cyclic_carve(const CyclicPlan &p, char *base, 
   CyclicDevResult *res = c.take<CyclicDevResult>(1);
   GridBarrierState *gb = c.take<GridBarrierState>(1);
   double *gpart = c.take<double>(2 * (p.grid_blocks > 1 ? p.grid_blocks : 1) * KR_RED_K);
+  double *Vc = nullptr, *Hb = nullptr, *Wb = nullptr, *Rk = nullptr, *Pk = nullptr, *Ak = nullptr, *Tk = nullptr;
+  if (p.block_polish) {
+    Vc = c.take<double>(KR_NBP * p.ldn);
+    Hb = c.take<double>(KR_NBP * p.ldm);
+    Wb = c.take<double>(KR_NBP * p.ldm);
+    Rk = c.take<double>(KR_NBP * p.ldm);
+    Pk = c.take<double>(KR_NBP * p.ldm);
+    Ak = c.take<double>(KR_NBP * p.ldm);
+    Tk = c.take<double>(KR_NBP * p.ldn);
+  }
   if (d) {
     d->Y = Y; d->X = X; d->wx = wx; d->wy = wy;
     if (p.own_basis) d->basis = basis;
@@ -130,6 +144,7 @@ __host__ __device__ inline size_t cyclic_carve(const CyclicPlan &p, char *base, 
     d->eig_cs = eig_cs; d->eig_pq = eig_pq; d->eig_ord = eig_ord;
     if (p.own_basis) { d->status = status; d->res = res; }
     d->gb = gb; d->gpart = gpart;
+    d->Vc = Vc; d->Hb = Hb; d->Wb = Wb; d->Rk = Rk; d->Pk = Pk; d->Ak = Ak; d->Tk = Tk;
     d->ldn = p.ldn; d->ldm = p.ldm; d->ldb = p.ldb; d->cap = p.cap;
   }
   return c.off + 256;

@@ -44,11 +44,11 @@ def small_mix(count=24, seed=3):
     return out
 
 
-@pytest.mark.parametrize("precision", [0, 1])
-def test_batch_accuracy(ctx, oracle, precision):
+@pytest.mark.parametrize("precision,polish_block", [(0, 0), (1, 0), (0, 1), (1, 1)])
+def test_batch_accuracy(ctx, oracle, precision, polish_block):
     from krans_b200.serving import solve_batch
     insts = small_mix()
-    reqs = make_requests(ctx, insts, precision)
+    reqs = make_requests(ctx, insts, precision, polish_block=polish_block)
     solve_batch(ctx, reqs)
     for inst, rq in zip(insts, reqs):
         r = rq.result

@@ -79,6 +79,20 @@ def test_golden_matrices(ctx, oracle, k):
     assert oracle.subspace_dist(O.right_null, U) < 1e-6
 
 
+@pytest.mark.parametrize("team", TEAMS)
+@pytest.mark.parametrize("k", [1, 5])
+def test_golden_matrices_block_polish(ctx, oracle, k, team):
+    """Block CG polish (up to 8 candidates per group): same acceptance bar and
+    the same subspace as the one-by-one polish."""
+    A, nul = load_golden_matrix(k)
+    R, U, _ = solve(ctx, A, 1, team=team, k=nul, polish_block=1)
+    assert U.shape[0] == nul and R.converged_to_target
+    thr = max(1e-12, 1e-10 * max(1.0, R.frob_norm_est))
+    assert max(np.linalg.norm(A @ u) for u in U) <= thr
+    assert oracle.max_pairwise_abs_dot(U) <= 1e-8
+    assert oracle.subspace_dist(dense_kernel(A, nul), U) < 1e-6
+
+
 def test_difference_operator_cg_limits(ctx):
     d = G.difference_operator(1000)
     R, U, _ = solve(ctx, d.A, 42)
