@@ -75,7 +75,7 @@ struct BatchLaunch {
     static const int cl_size = [] {
       const char *e = getenv("KRANS_CLUSTER_SIZE");
       int v = e ? atoi(e) : 8;
-      return (v == 2 || v == 4 || v == 8 || v == 16) ? v : 8;
+      return (v >= 2 && v <= 16) ? v : 8;
     }();
     csize = cl_size;
     auto is_large = [&](int a) { return reqs[a].A->m + reqs[a].A->n >= cluster_min && cluster_min > 0; };

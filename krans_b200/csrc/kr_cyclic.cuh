@@ -135,27 +135,33 @@ template <class Team, class KT> struct CyclicSolver {
   }
 
   // CG on (F F^T) w = rhs (CyclicLanczosSolver.cpp:48-113), no preconditioner.
-  __device__ __noinline__ int64_t cg(const double *rhs, double *w, int64_t maxit, double rel_tol, double bd_tol,
-                    double *rnorm_out) {
-    double *r = d.r, *p = d.p, *Ap = d.Ap, *tn = d.tn;
+  // The callers only use F^T w, so this returns u = F^T w instead of w: u
+  // accumulates alpha_k F^T p_k, and F^T p_k is the vector the first SpMV of
+  // iteration k forms anyway. The m-vector w and the closing F^T w product
+  // are never needed (same value in exact arithmetic; rounding differs).
+  // r and p are stored interleaved, so the gather of r + beta p at each entry
+  // of F^T is one 16-byte load.
+  __device__ __noinline__ int64_t cg(const double *rhs, double *u, int64_t maxit, double rel_tol, double bd_tol,
+                                     double *rnorm_out) {
+    double2 *rp = d.rp;
+    double *Ap = d.Ap, *tn = d.tn;
     double rr = 0.0;
+    team_for(tm, n, [&](int64_t i) { u[i] = 0.0; });
     team_for4(tm, m, [&](const int64_t *ix, int cnt) {
       double xv[4];
 #pragma unroll
-      for (int u = 0; u < 4; u++)
-        if (u < cnt)
-          xv[u] = rhs[ix[u]];
+      for (int u4 = 0; u4 < 4; u4++)
+        if (u4 < cnt)
+          xv[u4] = rhs[ix[u4]];
 #pragma unroll
-      for (int u = 0; u < 4; u++)
-        if (u < cnt) {
-          w[ix[u]] = 0.0;
-          r[ix[u]] = xv[u];
-          p[ix[u]] = xv[u];
-          rr += xv[u] * xv[u];
+      for (int u4 = 0; u4 < 4; u4++)
+        if (u4 < cnt) {
+          rp[ix[u4]] = make_double2(xv[u4], xv[u4]);
+          rr += xv[u4] * xv[u4];
         }
     });
     rr = tm.sum1(rr);
-    c.bytes += 32.0 * m;
+    c.bytes += 24.0 * m + 8.0 * n;
     const double rhsn = sqrt(rr > 0.0 ? rr : 0.0);
     *rnorm_out = rhsn;
     if (!(rhsn > 0.0) || !isfinite(rhsn))
@@ -177,15 +183,20 @@ template <class Team, class KT> struct CyclicSolver {
     for (; k < maxit && tm.ok(); ++k) {
       const double bq = beta;
       team_spmv_x(
-          tm, d.B.rows, d.B.rp, d.B.ci, d.B.v64, [&](int32_t cc) { return r[cc] + bq * p[cc]; }, d.B.lanes,
-          d.B.ulen, [&](int64_t i, double s) { tn[i] = s; });
+          tm, d.B.rows, d.B.rp, d.B.ci, d.B.v64,
+          [&](int32_t cc) {
+            const double2 q = rp[cc];
+            return q.x + bq * q.y;
+          },
+          d.B.lanes, d.B.ulen, [&](int64_t i, double s) { tn[i] = s; });
       count_B();
-      c.bytes += spmv_bytes(d.B.rows, d.B.cols, d.B.nnz, 8, 8, 8) + 8.0 * m;
+      c.bytes += spmv_bytes(d.B.rows, d.B.cols, d.B.nnz, 8, 16, 8);
       tm.sync();
       double pap = 0.0;
       csr_mv(tm, d.F, d.F.v64, tn, [&](int64_t i, double s) {
-        const double pn = r[i] + bq * p[i];
-        p[i] = pn;
+        const double2 q = rp[i];
+        const double pn = q.x + bq * q.y;
+        rp[i].y = pn;
         Ap[i] = s;
         pap += pn * s;
       });
@@ -197,26 +208,36 @@ template <class Team, class KT> struct CyclicSolver {
       const double alpha = rz / pap;
       double rzn = 0.0;
       team_for4(tm, m, [&](const int64_t *ix, int cnt) {
-        double pv[4], wv[4], rv[4], av[4];
+        double rv[4], av[4];
 #pragma unroll
-        for (int u = 0; u < 4; u++)
-          if (u < cnt) {
-            pv[u] = p[ix[u]];
-            wv[u] = w[ix[u]];
-            rv[u] = r[ix[u]];
-            av[u] = Ap[ix[u]];
+        for (int u4 = 0; u4 < 4; u4++)
+          if (u4 < cnt) {
+            rv[u4] = rp[ix[u4]].x;
+            av[u4] = Ap[ix[u4]];
           }
 #pragma unroll
-        for (int u = 0; u < 4; u++)
-          if (u < cnt) {
-            w[ix[u]] = wv[u] + alpha * pv[u];
-            const double ri = rv[u] - alpha * av[u];
-            r[ix[u]] = ri;
+        for (int u4 = 0; u4 < 4; u4++)
+          if (u4 < cnt) {
+            const double ri = rv[u4] - alpha * av[u4];
+            rp[ix[u4]].x = ri;
             rzn += ri * ri;
           }
       });
+      team_for4(tm, n, [&](const int64_t *ix, int cnt) {
+        double uv[4], tv[4];
+#pragma unroll
+        for (int u4 = 0; u4 < 4; u4++)
+          if (u4 < cnt) {
+            uv[u4] = u[ix[u4]];
+            tv[u4] = tn[ix[u4]];
+          }
+#pragma unroll
+        for (int u4 = 0; u4 < 4; u4++)
+          if (u4 < cnt)
+            u[ix[u4]] = uv[u4] + alpha * tv[u4];
+      });
       rzn = tm.sum1(rzn); // its barrier also publishes r for the next gather
-      c.bytes += 40.0 * m;
+      c.bytes += 24.0 * m + 24.0 * n;
       if (!isfinite(rzn))
         break;
       rnorm = sqrt(rzn > 0.0 ? rzn : 0.0);
@@ -393,10 +414,10 @@ template <class Team, class KT> struct CyclicSolver {
     scale(n, 1.0 / nv, v);
     const double tnorm = mulF_norm(v, tmv);
     double rn;
-    const int64_t its = cg(tmv, wm, 500, 1e-12, 1e-30, &rn);
+    double *u = d.vp;
+    const int64_t its = cg(tmv, u, 500, 1e-12, 1e-30, &rn);
     if (its > 0 || rn < tnorm) {
-      mulB(wm, tn);
-      team_for(tm, n, [&](int64_t i) { v[i] -= tn[i]; });
+      team_for(tm, n, [&](int64_t i) { v[i] -= u[i]; });
       tm.sync();
     }
     if (nb > 0) {
@@ -705,15 +726,14 @@ template <class Team, class KT> struct CyclicSolver {
           } else {
             double rn;
             const uint64_t t_cg1 = globaltimer_ns();
-            const int64_t cg_its = cg(tmv, wm, o.cg_maxit, o.cg_rel_tol, o.cg_breakdown_tol, &rn);
+            const int64_t cg_its = cg(tmv, vp, o.cg_maxit, o.cg_rel_tol, o.cg_breakdown_tol, &rn);
             c.t_cg += globaltimer_ns() - t_cg1;
             c.cg_solves++;
             if (cg_its >= o.cg_maxit) {
               c.cg_maxit_hits++;
               hit_maxit = true;
             }
-            mulB(wm, d.tn);
-            team_for(tm, n, [&](int64_t i) { vp[i] = v[i] - d.tn[i]; });
+            team_for(tm, n, [&](int64_t i) { vp[i] = v[i] - vp[i]; });
           }
           c.bytes += 24.0 * n;
           tm.sync();
@@ -934,15 +954,14 @@ template <class Team, class KT> struct CyclicSolver {
         for (int pass = 0; pass < passes && res > accept && tm.ok(); ++pass) {
           double rn;
           const uint64_t t_cg0 = globaltimer_ns();
-          cg_its = cg(tmv, wm, o.cg_maxit, o.cg_rel_tol, o.cg_breakdown_tol, &rn);
+          cg_its = cg(tmv, vp, o.cg_maxit, o.cg_rel_tol, o.cg_breakdown_tol, &rn); // vp = F^T w
           c.t_cg += globaltimer_ns() - t_cg0;
           c.cg_solves++;
           if (cg_its >= o.cg_maxit) {
             c.cg_maxit_hits++;
             hit_maxit = true;
           }
-          mulB(wm, tn);
-          team_for(tm, n, [&](int64_t i) { vp[i] = v[i] - tn[i]; });
+          team_for(tm, n, [&](int64_t i) { vp[i] = v[i] - vp[i]; });
           c.bytes += 24.0 * n;
           tm.sync();
           gs2_basis(vp);

@@ -376,9 +376,8 @@ template <> struct AccOf<double> { using T = double; };
 template <> struct AccOf<float> { using T = float; };
 
 // Thread-per-row SpMV for matrices whose rows all hold exactly L entries
-// (L == lanes): no row pointers, vector loads of the (column, value) pairs.
-// The products are combined with the same tree as the lane butterfly of
-// team_spmv_x, so both paths give bit-identical results.
+// (L = 1, 2 or 4): no row pointers, vector loads of the (column, value)
+// pairs. The products are combined with the tree of an L-lane butterfly.
 template <int L, class Team, class VT, class GX, class Epi>
 KR_DEV void team_spmv_uniform(Team &tm, int64_t rows, const int32_t *__restrict__ ci,
                               const VT *__restrict__ val, GX gx, Epi epi) {
@@ -465,7 +464,7 @@ KR_DEV void team_spmv_uniform(Team &tm, int64_t rows, const int32_t *__restrict_
 template <class Team, class VT, class GX, class Epi>
 KR_DEV void team_spmv_x(Team &tm, int64_t rows, const int32_t *__restrict__ rp, const int32_t *__restrict__ ci,
                         const VT *__restrict__ val, GX gx, int lanes, int32_t ulen, Epi epi) {
-  if (ulen == lanes) {
+  if (ulen == 1 || ulen == 2 || ulen == 4) {
     if (ulen == 2) {
       team_spmv_uniform<2>(tm, rows, ci, val, gx, epi);
       return;

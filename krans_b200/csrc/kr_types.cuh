@@ -66,7 +66,8 @@ struct CyclicDesc {
   double *y0, *v, *vp, *best_v, *tn; // n-vectors
   double *Vc;                        // KR_NBP candidate n-vectors (block polish)
   double *Hb, *Wb, *Rk, *Pk, *Ak, *Tk; // interleaved CG blocks: m x KR_NBP (Tk: n x KR_NBP)
-  double *tmv, *wm, *r, *p, *Ap;     // m-vectors
+  double *tmv, *wm, *Ap;             // m-vectors
+  double2 *rp;                       // CG residual and direction, interleaved (m)
   double *alpha, *beta;              // ncv + 2
   double *Tb, *Vt, *sv;              // tiny problem
   int32_t *ord;
@@ -113,8 +114,9 @@ __host__ __device__ inline size_t cyclic_carve(const CyclicPlan &p, char *base, 
   double *basis = p.own_basis ? c.take<double>((p.k_target > 1 ? p.k_target : 1) * p.ldb) : nullptr;
   double *y0 = c.take<double>(p.ldn), *v = c.take<double>(p.ldn), *vp = c.take<double>(p.ldn);
   double *best_v = c.take<double>(p.ldn), *tn = c.take<double>(p.ldn);
-  double *tmv = c.take<double>(p.ldm), *wm = c.take<double>(p.ldm), *r = c.take<double>(p.ldm);
-  double *pp = c.take<double>(p.ldm), *Ap = c.take<double>(p.ldm);
+  double *tmv = c.take<double>(p.ldm), *wm = c.take<double>(p.ldm);
+  double2 *rp = c.take<double2>(p.ldm);
+  double *Ap = c.take<double>(p.ldm);
   double *alpha = c.take<double>(p.ncv + 2), *beta = c.take<double>(p.ncv + 2);
   double *Tb = c.take<double>((p.ncv + 1) * p.ncv), *Vt = c.take<double>(p.ncv * p.ncv);
   double *sv = c.take<double>(p.ncv + 1);
@@ -139,7 +141,7 @@ __host__ __device__ inline size_t cyclic_carve(const CyclicPlan &p, char *base, 
     d->Y = Y; d->X = X; d->wx = wx; d->wy = wy;
     if (p.own_basis) d->basis = basis;
     d->y0 = y0; d->v = v; d->vp = vp; d->best_v = best_v; d->tn = tn;
-    d->tmv = tmv; d->wm = wm; d->r = r; d->p = pp; d->Ap = Ap;
+    d->tmv = tmv; d->wm = wm; d->rp = rp; d->Ap = Ap;
     d->alpha = alpha; d->beta = beta; d->Tb = Tb; d->Vt = Vt; d->sv = sv; d->ord = ord;
     d->eig_cs = eig_cs; d->eig_pq = eig_pq; d->eig_ord = eig_ord;
     if (p.own_basis) { d->status = status; d->res = res; }
