@@ -40,6 +40,9 @@ WORKLOAD = "batched uneven null-space solves: 4096 instances (half shift operato
            "n log-uniform in [1e3, 2e5]; k = kernel dimension"
 
 
+METRIC = "null-space solves/s (p50/p99 latency, max||Au||/||A||<=1e-12) vs plain FP64 GPU"
+
+
 def lower_norm_bound(A) -> float:
     A2 = A.multiply(A)
     return float(np.sqrt(max(A2.sum(axis=0).max(), A2.sum(axis=1).max())))
@@ -126,14 +129,10 @@ def measured_peak():
     return 6650.0, "fallback"
 
 
-def profiled_traffic():
-    """dram bytes per launch of the batched kernels from the committed ncu
-    summary (profiles/batch_traffic.json), scaled to this bench's launch."""
-    p = os.path.join(ROOT, "profiles", "batch_traffic.json")
-    if not os.path.exists(p):
-        return None
-    with open(p) as f:
-        return json.load(f)
+# DRAM bytes (read + write) per algorithmic byte of the batched launch, from
+# one ncu capture of a 64-instance batch (larger than L2):
+# profiles/batched_launch_list_batch256.md. `traffic` scales it to this launch.
+DRAM_PER_ALGO_BYTE = 1.607e12 / 3.966e12
 
 
 # ---------------------------------------------------------------------------
@@ -185,10 +184,16 @@ def run_reference(args):
     solved = 0
     with ctx.Pool(cores) as pool:
         for s, insts in enumerate(batches):
-            # bounded sample: the smallest-first prefix of a stratified sample
+            # bounded sample: stratified by nnz over the smaller 75% of the
+            # batch (the largest quarter takes minutes per instance on one
+            # core); warm-up steps run the smallest instance only (the CPU
+            # path has nothing to warm beyond the page cache)
             order = sorted(range(len(insts)), key=lambda i: insts[i].A.nnz)
+            order = order[: max(1, (3 * len(order)) // 4)]
             stride = max(1, len(order) // max(1, args.ref_sample))
-            pick = [order[i] for i in range(0, len(order), stride)][: args.ref_sample]
+            pick = [order[i] for i in range(stride // 2, len(order), stride)][: args.ref_sample]
+            if s < args.warmup:
+                pick = order[:1]
             jobs = [((insts[i].A.shape[0], insts[i].A.shape[1], insts[i].A.indptr, insts[i].A.indices,
                       insts[i].A.data), insts[i].k, 1000 + i) for i in pick]
             t = time.perf_counter()
@@ -201,13 +206,13 @@ def run_reference(args):
     T = sum(p[1] for p in per_step)
     v = n / T if T > 0 else 0.0
     line = {
-        "impl": "reference", "metric": "null-space solves/s", "value": v, "unit": "solves/s",
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "solves/s",
         "higher_is_better": True, "n_gpus": 0, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * T / max(1, len(per_step)), "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "batch": args.batch, "sample_per_step": args.ref_sample},
+        "config": dict(batched_config(args, 1), sample_per_step=args.ref_sample),
         "cpu_baseline": {"value": v, "unit": "solves/s", "cores": cores, "kind": "port",
-                         "sample": f"{args.ref_sample} stratified instances per step of {args.batch}, "
-                                   f"one process per core"},
+                         "sample": f"{args.ref_sample} instances per step, stratified by nnz over the smaller "
+                                   f"75% of each {args.batch}-instance batch, one process per core"},
         "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "converged": solved, "vs_baseline": None,
     }
@@ -216,6 +221,12 @@ def run_reference(args):
 
 
 # ---------------------------------------------------------------------------
+def batched_config(args, world):
+    return {"workload": WORKLOAD, "batch_per_step": args.batch, "form": "mixed-precision batched",
+            "accept": "tol_abs=1e-12*max(row,col norm), tol_rel=0, cg_maxit=1000",
+            "l2": "each step a different ~1 GB batch (> L2)", "parallelism": f"replicas x{world}"}
+
+
 def run_ours(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -342,23 +353,18 @@ def run_ours(args):
     # ---- roofline of the batched launch
     peak, peak_kind = measured_peak()
     achieved = algo_bytes / (sum(dev_ms) / 1e3) / 1e9 if dev_ms else 0.0
-    prof = profiled_traffic()
-    traffic = None
-    if prof and prof.get("bytes_per_algo_byte"):
-        traffic = prof["bytes_per_algo_byte"] * algo_bytes / max(1, len(dev_ms))
+    traffic = DRAM_PER_ALGO_BYTE * algo_bytes / max(1, len(dev_ms))
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                 "kernel": "cyclic_batch_kernel + cyclic_batch_cluster_kernel (one launch per step)",
                 "algo_bytes_per_launch": algo_bytes / max(1, len(dev_ms))}
 
     line = {
-        "metric": "null-space solves/s (p50/p99 latency, max||Au||/||A||<=1e-12) vs plain FP64 GPU",
+        "metric": METRIC,
         "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * T / max(1, args.steps), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 SpMV/Krylov + f64 reorth/tiny-SVD/CG polish", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "batch_per_step": args.batch, "form": "mixed-precision batched",
-                   "accept": "tol_abs=1e-12*max(row,col norm), tol_rel=0, cg_maxit=1000",
-                   "l2": "each step a different ~1 GB batch (> L2)", "parallelism": f"replicas x{world}"},
+        "config": batched_config(args, world),
         "latency_ms": {"p50": percentile(lat, 50), "p99": percentile(lat, 99),
                        "definition": "launch start -> request done, device clock"},
         "accuracy": {"converged": ok_all, "solves": nsolves_all, "max_rel_residual": worst},
@@ -383,6 +389,310 @@ def run_ours(args):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# Other workloads (python bench.py --workload NAME). The default run is the
+# batched one above; these print one JSON line each with their own metric.
+def _clocked(fn):
+    with ClockSampler(0) as clk:
+        out = fn()
+    return out, clk.summary()
+
+
+def run_quickstart(args):
+    """The quickstart instance (shift operator n=1000, N=3, c=0.5, k=3):
+    cyclic Lanczos then LOBPCG on one seeded factory (MT19937, seed 42), as the
+    reference's example runs them. Reports device microseconds per solve, and
+    end to end through the public API from host CSR arrays."""
+    import krans_b200 as kb
+    from krans_b200 import generators as G
+    from oracle import oracle as O
+    ctx = kb.Context(0)
+    inst = G.shift_operator(1000, 3, 0.5)
+    A = inst.A
+    cyc, lob, e2e, dists = [], [], [], []
+
+    def loop():
+        for it in range(args.warmup + args.steps):
+            t0 = time.perf_counter()
+            M = kb.CudaCsrMatrixAdapter(ctx, A.shape[0], A.shape[1], A.indptr, A.indices, A.data)
+            vf = kb.CudaVectorFactory(ctx, 1000, seed=42)
+            Rc = kb.find_nullspace_cyclic_lanczos_ex(M, vf, kb.CyclicLanczosOptions(k=3))
+            Uc = kb.basis_to_numpy(Rc.right_null)
+            Rl = kb.find_nullspace_lobpcg_ex(M, vf, kb.LOBPCGOptions(nev=3))
+            Ul = kb.basis_to_numpy(Rl.right_null)
+            t1 = time.perf_counter()
+            if it >= args.warmup:
+                cyc.append(Rc.device_ms * 1e3)
+                lob.append(Rl.device_ms * 1e3)
+                e2e.append((t1 - t0) * 1e6)
+                dists.append(max(O.subspace_dist(inst.kernel, Uc), O.subspace_dist(inst.kernel, Ul)))
+    O.build()
+    _, clocks = _clocked(loop)
+    Ao = O.Csr.from_scipy(A)
+    tc, tl = [], []
+    for _ in range(5):
+        rng = O.Rng(42)
+        t0 = time.perf_counter()
+        O.cyclic(Ao, rng, k=3)
+        t1 = time.perf_counter()
+        O.lobpcg(Ao, rng, nev=3)
+        t2 = time.perf_counter()
+        tc.append((t1 - t0) * 1e6)
+        tl.append((t2 - t1) * 1e6)
+    med = statistics.median
+    v = med(cyc) + med(lob)
+    line = {
+        "metric": "quickstart latency: cyclic Lanczos (k=3) + LOBPCG (nev=3) on one seeded factory",
+        "value": v, "unit": "us", "higher_is_better": False, "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": v / 1e3, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "shift operator n=1000, N=3, c=0.5 (the reference's quickstart), k=3",
+                   "l2": "resident (44 KB problem; latency-bound)"},
+        "cyclic_us": med(cyc), "lobpcg_us": med(lob), "max_subspace_dist": max(dists),
+        "e2e": {"value": med(e2e), "unit": "us",
+                "h2d_bytes_per_step": int(A.data.nbytes + A.indices.nbytes + A.indptr.nbytes),
+                "d2h_bytes_per_step": 6 * 1000 * 8},
+        "cpu_baseline": {"value": med(tc) + med(tl), "unit": "us", "cores": 1, "kind": "port",
+                         "cyclic_us": med(tc), "lobpcg_us": med(tl),
+                         "sample": "the same instance, C oracle, 5 repetitions"},
+        "clocks": clocks, "gpu_launches": 2 * args.steps,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def kernel_dist_indicator(U, labels, ncomp):
+    """Largest principal-angle sine between the rows of U (orthonormal) and the
+    span of the component indicator vectors given by `labels`."""
+    cnt = np.bincount(labels, minlength=ncomp).astype(np.float64)
+    R = np.empty_like(U)
+    for i in range(U.shape[0]):
+        mean = np.bincount(labels, weights=U[i], minlength=ncomp) / np.maximum(cnt, 1)
+        R[i] = U[i] - mean[labels]
+    return float(np.linalg.norm(R, 2)) if U.shape[0] == ncomp else 1.0
+
+
+def run_lobpcg_incidence(args):
+    """Large LOBPCG solve: graph incidence matrix of 64 components x 2^s
+    vertices (s = --scale; 16 is the full 4,194,304-vertex case), mean degree 8,
+    nev = k = 64, block_size = 96, tol_abs = 1e-12 L, tol_rel = 0."""
+    import krans_b200 as kb
+    from krans_b200 import generators as G
+    ctx = kb.Context(0)
+    comps = 64
+    nv = comps << args.scale
+    inst = G.graph_incidence(nv, comps, 8.0, seed=1, kernel=False)
+    A = inst.A
+    L = lower_norm_bound(A)
+    M = kb.CudaCsrMatrixAdapter.from_scipy(ctx, A)
+    small = G.graph_incidence(comps << 8, comps, 8.0, seed=2, kernel=False)
+    Ms = kb.CudaCsrMatrixAdapter.from_scipy(ctx, small.A)
+    for _ in range(max(1, args.warmup)):
+        kb.find_nullspace_lobpcg_ex(Ms, kb.CudaVectorFactory(ctx, small.A.shape[1], seed=3),
+                                    kb.LOBPCGOptions(nev=comps, block_size=96, max_iters=50))
+    opt = kb.LOBPCGOptions(nev=comps, block_size=96, tol_abs=1e-12 * L, tol_rel=0.0,
+                           max_iters=args.max_iters)
+
+    def solve():
+        R = kb.find_nullspace_lobpcg_ex(M, kb.CudaVectorFactory(ctx, A.shape[1], seed=42), opt)
+        return R, kb.basis_to_numpy(R.right_null)
+    (R, U), clocks = _clocked(solve)
+    from scipy.sparse.csgraph import connected_components
+    ncomp, labels = connected_components((A.T @ A).tocsr(), directed=False)
+    worst = max((float(np.linalg.norm(A @ u)) for u in U), default=float("nan")) / L
+    dist = kernel_dist_indicator(U, labels, ncomp) if U.shape[0] else 1.0
+    T = R.device_ms / 1e3
+    peak = measured_peak()[0]
+    line = {
+        "metric": "large LOBPCG null-space solve time (k=64, bs=96)", "value": T, "unit": "s",
+        "higher_is_better": False, "n_gpus": 1, "steps": 1, "warmup": args.warmup, "ms_per_step": 1e3 * T,
+        "scaling": "strong", "vs_baseline": None, "dtype": "f64 (Gram on FP64 tensor cores)",
+        "data": "synthetic",
+        "config": {"workload": f"graph incidence, {comps} components x 2^{args.scale} vertices, mean degree 8",
+                   "m": A.shape[0], "n": A.shape[1], "nnz": A.nnz, "nev": comps, "block_size": 96,
+                   "accept": "tol_abs=1e-12*max(row,col norm), tol_rel=0", "max_iters": args.max_iters},
+        "iters": R.iters, "found": U.shape[0], "converged": R.converged_to_target,
+        "max_rel_residual": worst, "subspace_dist_to_kernel": dist,
+        "roofline": {"bound": "hbm", "achieved": R.algo_bytes / T / 1e9, "peak": peak,
+                     "unit": "GB/s", "frac": R.algo_bytes / T / 1e9 / peak, "traffic": None},
+        "gram_tflops": R.gram_flops / T / 1e12,
+        "phase_ms": {"apply_normal": R.phase_ms[0], "gram": R.phase_ms[1], "tiny_gep": R.phase_ms[2],
+                     "orthonormalise": R.phase_ms[3], "rest": R.phase_ms[4]},
+        "clocks": clocks, "gpu_launches": 1,
+    }
+    if not args.no_cpu_baseline:
+        from oracle import oracle as O
+        O.build()
+        cs = G.graph_incidence(comps << args.cpu_scale, comps, 8.0, seed=1, kernel=False)
+        t0 = time.perf_counter()
+        Ro = O.lobpcg(O.Csr.from_scipy(cs.A), O.Rng(42), nev=comps, block_size=96,
+                      tol_abs=1e-12 * lower_norm_bound(cs.A), tol_rel=0.0, max_iters=args.cpu_iters)
+        dt = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": dt / max(1, Ro.iters), "unit": "s per LOBPCG iteration", "cores": 1,
+                                "kind": "port",
+                                "sample": f"{args.cpu_iters} iterations on 64 x 2^{args.cpu_scale} vertices "
+                                          f"(n={cs.A.shape[1]}); the GPU figure per iteration is "
+                                          f"{T / max(1, R.iters):.4g} s at n={A.shape[1]}"}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_planted(args):
+    """Planted-kernel cyclic Lanczos solve: A = [B | B W], B m x (n-k) with 8
+    N(0,1) entries per row, W (n-k) x k with 4 per column; full size m=3e6,
+    n-k=2e6, k=32, divided by 2^(16 - --scale) per dimension (k stays 32).
+    Mixed precision (FP32 SpMV/Lanczos, FP64 reorth/tiny SVD/polish)."""
+    import krans_b200 as kb
+    from krans_b200 import generators as G
+    ctx = kb.Context(0)
+    div = 1 << max(0, 16 - args.scale)
+    m, nk, k = 3_000_000 // div, 2_000_000 // div, 32
+    inst = G.planted_kernel(m, nk, k, seed=1, kernel=False)
+    A = inst.A
+    L = lower_norm_bound(A)
+    M = kb.CudaCsrMatrixAdapter.from_scipy(ctx, A, fp32=True)
+    opt = kb.CyclicLanczosOptions(k=k, tol_abs=1e-12 * L, tol_rel=0.0, cg_maxit=1000, ncv=args.ncv,
+                                  max_restarts=args.max_restarts, precision=kb.Precision.MIXED)
+
+    def solve():
+        R = kb.find_nullspace_cyclic_lanczos_ex(M, kb.CudaVectorFactory(ctx, A.shape[1], seed=42, mode="philox"),
+                                                opt)
+        return R, kb.basis_to_numpy(R.right_null)
+    (R, U), clocks = _clocked(solve)
+    worst = max((float(np.linalg.norm(A @ u)) for u in U), default=float("nan")) / L
+    T = R.device_ms / 1e3
+    peak = measured_peak()[0]
+    line = {
+        "metric": "planted-kernel cyclic Lanczos solve time (k=32, mixed precision)", "value": T, "unit": "s",
+        "higher_is_better": False, "n_gpus": 1, "steps": 1, "warmup": 0, "ms_per_step": 1e3 * T,
+        "scaling": "strong", "vs_baseline": None, "dtype": "f32 SpMV/Krylov + f64 reorth/tiny-SVD/CG polish",
+        "data": "synthetic",
+        "config": {"workload": f"planted kernel A=[B|BW], m={m}, n={A.shape[1]}, k={k}", "nnz": A.nnz,
+                   "ncv": args.ncv, "max_restarts": args.max_restarts,
+                   "accept": "tol_abs=1e-12*max(row,col norm), tol_rel=0, cg_maxit=1000"},
+        "found": U.shape[0], "converged": R.converged_to_target, "restarts": R.restarts,
+        "cg_solves": R.cg_solves, "max_rel_residual": worst,
+        "roofline": {"bound": "hbm", "achieved": R.algo_bytes / T / 1e9, "peak": peak,
+                     "unit": "GB/s", "frac": R.algo_bytes / T / 1e9 / peak, "traffic": None},
+        "phase_ms": list(R.phase_ms), "clocks": clocks, "gpu_launches": 1,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def serving_pool(P, nnz_lo, nnz_hi, seed=7):
+    """Request matrices of the serving stream: shift and incidence operators
+    (mean degree 6, as in the batched workload), incidence of mean degree 8 and
+    planted kernels, nnz log-uniform in [nnz_lo, nnz_hi]."""
+    from krans_b200 import generators as G
+    out = []
+    for i in range(P):
+        r = np.random.Generator(np.random.PCG64([seed, i]))
+        nnz = float(np.exp(r.uniform(np.log(nnz_lo), np.log(nnz_hi))))
+        kind = i % 4
+        if kind == 0:
+            N = int(r.integers(1, 17))
+            out.append(G.shift_operator(max(int(nnz / 2), 64), N, float(r.uniform(0.3, 0.9)), kernel=False))
+        elif kind in (1, 2):
+            deg = 6.0 if kind == 1 else 8.0
+            comps = int(r.integers(1, 17))
+            out.append(G.graph_incidence(max(int(nnz / deg), 4 * comps), comps, deg,
+                                         seed=int(r.integers(1 << 31)), kernel=False))
+        else:
+            k = int(r.integers(1, 9))
+            nk = max(int(nnz / 13), 64)
+            out.append(G.planted_kernel(int(1.5 * nk), nk, k, seed=int(r.integers(1 << 31)), kernel=False))
+    return out
+
+
+def _stream(ctx, pool, mats, rate, seconds, precision, max_inflight, max_batch, seed):
+    """Poisson arrivals at `rate`/s for `seconds`; each request draws a pool
+    matrix. Requests still unfinished when the window closes are cancelled
+    (queued) or drained (running) and do not count as completed."""
+    import krans_b200 as kb
+    from krans_b200.serving import Server, SolveRequest
+    rng = np.random.default_rng(seed)
+    srv = Server(ctx, max_inflight=max_inflight, max_batch=max_batch)
+    pending = {}
+    lat = []
+    done = ok = offered = 0
+    t0 = time.perf_counter()
+    nxt = rng.exponential(1.0 / rate)
+    while True:
+        now = time.perf_counter() - t0
+        if now >= seconds:
+            break
+        while nxt <= now:
+            i = int(rng.integers(len(pool)))
+            inst = pool[i]
+            o = kb.CyclicLanczosOptions(k=inst.k, tol_abs=1e-12 * lower_norm_bound(inst.A), tol_rel=0.0,
+                                        cg_maxit=1000, precision=kb.Precision(precision))
+            rq = SolveRequest(mats[i], o, seed=offered + 1)
+            pending[srv.submit(rq)] = rq
+            offered += 1
+            nxt += rng.exponential(1.0 / rate)
+        for t in list(pending):
+            st, res = srv.poll(t)
+            if st in ("done", "failed"):
+                pending.pop(t)
+                done += 1
+                ok += int(st == "done" and res.converged_to_target)
+                lat.append(res.latency_ms)
+        time.sleep(0.002)
+    elapsed = time.perf_counter() - t0
+    unfinished = len(pending)
+    from krans_b200._capi import KransError
+    for t in list(pending):
+        try:
+            srv.cancel(t)  # still queued
+        except KransError:
+            pass           # already running: drained below
+    srv.drain(600.0)
+    srv.close()
+    return {"offered": offered, "completed": done, "converged": ok, "window_s": elapsed,
+            "sustained_solves_per_s": done / elapsed,
+            "p50_ms": percentile(lat, 50), "p99_ms": percentile(lat, 99), "unfinished": unfinished}
+
+
+def run_serving(args):
+    """Serving stream: Poisson arrivals into the continuous-batching server
+    (mixed precision, HBM budget 150 GB) at an offered load below its measured
+    capacity and at an oversubscribed one; the plain FP64 one-at-a-time path
+    on the same stream as the baseline."""
+    import krans_b200 as kb
+    from krans_b200.serving import SolveRequest, solve_batch
+    ctx = kb.Context(0)
+    pool = serving_pool(args.pool, args.nnz_lo, args.nnz_hi)
+    mats = [kb.CudaCsrMatrixAdapter.from_scipy(ctx, inst.A, fp32=True) for inst in pool]
+    # capacity of the batched mixed form on this pool (one launch over it)
+    reqs = [SolveRequest(M, kb.CyclicLanczosOptions(k=i.k, tol_abs=1e-12 * lower_norm_bound(i.A), tol_rel=0.0,
+                                                    cg_maxit=1000, precision=kb.Precision.MIXED), seed=j + 1)
+            for j, (i, M) in enumerate(zip(pool, mats))]
+    solve_batch(ctx, reqs)
+    ms = solve_batch(ctx, reqs)
+    cap = len(reqs) / (ms / 1e3)
+    low, clk_low = _clocked(lambda: _stream(ctx, pool, mats, 0.5 * cap, args.seconds, 1, 4, 1024, 11))
+    high, clk_high = _clocked(lambda: _stream(ctx, pool, mats, 4.0 * cap, args.seconds, 1, 4, 1024, 12))
+    base = _stream(ctx, pool, mats, 0.5 * cap, args.seconds, 0, 1, 1, 11)
+    line = {
+        "metric": "serving stream: sustained null-space solves/s and p50/p99 latency incl. queueing",
+        "value": high["sustained_solves_per_s"], "unit": "solves/s", "higher_is_better": True, "n_gpus": 1,
+        "steps": 1, "warmup": 1, "ms_per_step": 1e3 * args.seconds, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 SpMV/Krylov + f64 reorth/tiny-SVD/CG polish", "data": "synthetic",
+        "config": {"workload": f"Poisson arrivals over a pool of {args.pool} matrices (shift, incidence deg 6/8, "
+                               f"planted k<=8), nnz log-uniform [{args.nnz_lo:.0e}, {args.nnz_hi:.0e}]",
+                   "seconds_per_phase": args.seconds, "hbm_budget_gb": 150,
+                   "batched_capacity_solves_per_s": cap},
+        "below_capacity": dict(low, offered_rate=0.5 * cap, clocks=clk_low),
+        "oversubscribed": dict(high, offered_rate=4.0 * cap),
+        "plain_fp64_one_at_a_time": dict(base, offered_rate=0.5 * cap),
+        "clocks": clk_high, "gpu_launches": None,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -395,11 +705,26 @@ def main():
     ap.add_argument("--ref-sample", type=int, default=16)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", choices=["batched", "quickstart", "lobpcg", "planted", "serving"],
+                    default="batched")
+    ap.add_argument("--scale", type=int, default=16, help="lobpcg/planted: log2 size (16 = full)")
+    ap.add_argument("--max-iters", type=int, default=1000)
+    ap.add_argument("--cpu-scale", type=int, default=10)
+    ap.add_argument("--cpu-iters", type=int, default=3)
+    ap.add_argument("--ncv", type=int, default=96)
+    ap.add_argument("--max-restarts", type=int, default=400)
+    ap.add_argument("--pool", type=int, default=64)
+    ap.add_argument("--nnz-lo", type=float, default=1e4)
+    ap.add_argument("--nnz-hi", type=float, default=2e6)
+    ap.add_argument("--seconds", type=float, default=20.0)
     args = ap.parse_args()
     if args.warmup < 3:
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload != "batched":
+        return {"quickstart": run_quickstart, "lobpcg": run_lobpcg_incidence, "planted": run_planted,
+                "serving": run_serving}[args.workload](args)
     return run_ours(args)
 
 

@@ -215,6 +215,8 @@ typedef struct krans_lobpcg_result {
   int64_t spmv, spmvT;
   double algo_bytes, gram_flops;
   double device_ms;
+  double phase_ms[5]; /* device time (ms): apply_normal (SpMV pairs), Gram, tiny GEP,
+                         orthonormalisation, the rest */
 } krans_lobpcg_result;
 
 int krans_cyclic_opts_init(krans_cyclic_opts *o);

@@ -377,6 +377,7 @@ class LOBPCGResult:
     algo_bytes: float = 0.0
     gram_flops: float = 0.0
     device_ms: float = 0.0
+    phase_ms: tuple = ()
 
 
 def _require(A, vf):
@@ -450,7 +451,8 @@ def find_nullspace_lobpcg_ex(A: CudaCsrMatrixAdapter, vf: CudaVectorFactory,
         accept_threshold=res.accept_threshold,
         best_unaccepted_residual=res.best_unaccepted_residual, block_size=res.block_size,
         converged_to_target=bool(res.converged_to_target), spmv=res.spmv, spmvT=res.spmvT,
-        algo_bytes=res.algo_bytes, gram_flops=res.gram_flops, device_ms=res.device_ms)
+        algo_bytes=res.algo_bytes, gram_flops=res.gram_flops, device_ms=res.device_ms,
+        phase_ms=tuple(res.phase_ms))
 
 
 def find_nullspace_lobpcg(A, vf, opt) -> List[CudaVectorAdapter]:

@@ -25,6 +25,8 @@ template <class Team> struct LobpcgSolver {
   int64_t m, n, ldn;
   Counters c;
   double gram_flops = 0.0;
+  uint64_t t_ph[4] = {0, 0, 0, 0}; // apply_normal, Gram, tiny GEP, orthonormalisation (ns)
+  int orth_depth = 0;
   int err = 0;
 
   KR_DEV LobpcgSolver(Team &t, const LobpcgDesc &dd) : tm(t), d(dd) {
@@ -114,6 +116,14 @@ template <class Team> struct LobpcgSolver {
 
   // MGS with optional reorth (GramSchmidt.cpp:55-82) on k columns of block V.
   __device__ __noinline__ bool mgs(double *V, int64_t k, double tol, bool reorth) {
+    const uint64_t t0 = globaltimer_ns();
+    orth_depth++;
+    const bool ok = mgs_cols(V, k, tol, reorth);
+    if (--orth_depth == 0)
+      t_ph[3] += globaltimer_ns() - t0;
+    return ok;
+  }
+  __device__ __noinline__ bool mgs_cols(double *V, int64_t k, double tol, bool reorth) {
     for (int64_t i = 0; i < k; i++) {
       double *vi = col(V, i);
       gs_pass(V, i, vi);
@@ -137,6 +147,15 @@ template <class Team> struct LobpcgSolver {
   // back only on success.
   __device__ __noinline__ bool orthonormalize_block(double *Xb, int64_t k, const double *basis, int64_t nb, double tol,
                                    bool reorth, double *scratch) {
+    const uint64_t t0 = globaltimer_ns();
+    orth_depth++;
+    const bool ok = orthonormalize_cols(Xb, k, basis, nb, tol, reorth, scratch);
+    if (--orth_depth == 0)
+      t_ph[3] += globaltimer_ns() - t0;
+    return ok;
+  }
+  __device__ __noinline__ bool orthonormalize_cols(double *Xb, int64_t k, const double *basis, int64_t nb, double tol,
+                                                   bool reorth, double *scratch) {
     for (int64_t i = 0; i < k; i++) {
       double *xi = col(Xb, i);
       gs_pass(basis, nb, xi);
@@ -155,14 +174,18 @@ template <class Team> struct LobpcgSolver {
   }
 
   __device__ __noinline__ void apply_normal(const double *Zb, int64_t k, double *AZb) {
+    const uint64_t t0 = globaltimer_ns();
     for (int64_t j = 0; j < k; j++) {
       mulA(col((double *)Zb, j), d.tmv);
       mulAT(d.tmv, col(AZb, j));
     }
+    t_ph[0] += globaltimer_ns() - t0;
   }
 
   __device__ __noinline__ void form_gram(const double *Zb, const double *AZb, int p) {
+    const uint64_t t0 = globaltimer_ns();
     team_gram2(tm, n, Zb, AZb, ldn, p, d.S, d.G, d.gram_part);
+    t_ph[1] += globaltimer_ns() - t0;
     gram_flops += 2.0 * 2.0 * (double)n * p * p;
     c.bytes += 2.0 * 8.0 * n * p;
   }
@@ -170,9 +193,11 @@ template <class Team> struct LobpcgSolver {
   // solve_tiny_gep (LOBPCGSolver.cpp:88-119) on the leader block; theta in
   // d.th, eigenvectors in d.Ym (ld p). Returns false if S is not SPD.
   __device__ __noinline__ bool tiny_gep(int p) {
+    const uint64_t t0 = globaltimer_ns();
     if (tm.lead_cta())
       gep_block(p);
     tm.publish();
+    t_ph[2] += globaltimer_ns() - t0;
     return *(volatile int32_t *)d.flag == 0;
   }
   __device__ __noinline__ void gep_block(int p) {
@@ -432,6 +457,7 @@ template <class Team> struct LobpcgSolver {
     R.block_size = bs;
     double *X = d.X, *AX = d.AX, *Rb = d.Rb, *W = d.W, *P = d.P, *T1 = d.T1, *T2 = d.T2;
     int64_t nlocked = 0, nright = 0, its = 0;
+    const uint64_t t_run0 = globaltimer_ns();
 
     // ||A||_F estimate (LOBPCGSolver.cpp:163-178)
     {
@@ -659,6 +685,13 @@ template <class Team> struct LobpcgSolver {
       R.spmvT = c.spmvT;
       R.bytes = c.bytes;
       R.gram_flops = gram_flops;
+      const double tot = (double)(globaltimer_ns() - t_run0) * 1e-6;
+      double acc = 0.0;
+      for (int i = 0; i < 4; i++) {
+        R.phase_ms[i] = (double)t_ph[i] * 1e-6;
+        acc += R.phase_ms[i];
+      }
+      R.phase_ms[4] = tot - acc;
       *d.res = R;
     }
   }

@@ -173,6 +173,7 @@ struct LobpcgDevResult {
   int32_t err_code, pad;
   int64_t spmv, spmvT;
   double bytes, gram_flops;
+  double phase_ms[5]; // device time in: apply_normal, Gram, tiny GEP, orthonormalisation, the rest
 };
 
 // error codes of the reference's throws (reported as KRANS_ERR_RUNTIME)
