@@ -224,6 +224,235 @@ KR_DEV void block_jacobi_eig(int n, double *A, double *w, double *Q, double *rot
   __syncthreads();
 }
 
+// Block-wide sum of one value per thread; every thread receives the total
+// (fixed order: warp butterfly, then warps in index order). `red` is shared
+// scratch of KR_MAX_WARPS doubles.
+KR_DEV double blk_allsum(double v, double *red) {
+  v = warp_sum(v);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  __syncthreads();
+  if (lane == 0)
+    red[wid] = v;
+  __syncthreads();
+  double t = 0.0;
+  for (int i = 0; i < nw; i++)
+    t += red[i];
+  return t;
+}
+
+#define KR_EIG_MAX 512
+
+// Symmetric eigendecomposition of A (n x n, column-major, ld n; both
+// triangles referenced, destroyed) on one thread block: Householder reduction
+// to tridiagonal form with the orthogonal factor accumulated explicitly, then
+// the implicit QL algorithm with shifts for the tridiagonal matrix (Golub &
+// Van Loan, Matrix Computations, 4th ed., 8.3.1 and 8.3.3; QL as in Bowdler,
+// Martin, Reinsch and Wilkinson, Numer. Math. 11 (1968) 293-306). One thread
+// runs the scalar recurrence of each QL sweep into shared arrays of rotations;
+// all threads then apply the sweep to the rows of Z in parallel (the rows are
+// independent). w ascending (ties keep index order), Z columns = eigenvectors.
+// Returns 0, or nonzero if n > KR_EIG_MAX or an eigenvalue needed more than 60
+// sweeps (the caller then falls back to Jacobi).
+KR_DEV int block_sym_eig_ql(int n, double *A, double *w, double *Z, int *ord) {
+  __shared__ double s_d[KR_EIG_MAX], s_e[KR_EIG_MAX], s_c[KR_EIG_MAX], s_s[KR_EIG_MAX];
+  __shared__ double s_red[KR_MAX_WARPS];
+  __shared__ int s_m, s_lo, s_fail;
+  __shared__ double s_tn;
+  const int tid = threadIdx.x, bd = blockDim.x, lane = tid & 31, wid = tid >> 5, nw = bd >> 5;
+  if (n > KR_EIG_MAX || n < 1)
+    return -1;
+  // ---- 1) Householder reduction: column k below the subdiagonal -> alpha e1
+  for (int k = 0; k + 2 < n; k++) {
+    const int r0 = k + 1, r = n - r0;
+    double *x = A + r0 + (size_t)k * n; // A[r0:n, k]; becomes the Householder vector
+    double t2 = 0.0;
+    for (int i = 1 + tid; i < r; i += bd)
+      t2 += x[i] * x[i];
+    t2 = blk_allsum(t2, s_red);
+    const double x0 = x[0];
+    if (!(t2 > 0.0)) { // nothing to annihilate: H_k = I
+      if (tid == 0) {
+        s_d[k] = A[k + (size_t)k * n];
+        s_e[k] = x0;
+        s_s[k] = 0.0;
+      }
+      __syncthreads();
+      continue;
+    }
+    const double sig = sqrt(x0 * x0 + t2);
+    const double alpha = x0 >= 0.0 ? -sig : sig;
+    const double beta = 1.0 / (sig * (sig + fabs(x0))); // H = I - beta v v^T, v = x - alpha e1
+    __syncthreads();
+    if (tid == 0) {
+      x[0] = x0 - alpha;
+      s_d[k] = A[k + (size_t)k * n];
+      s_e[k] = alpha;
+      s_s[k] = beta;
+    }
+    __syncthreads();
+    // p = beta * A_sub v (A_sub symmetric: row i read as column i, coalesced)
+    double *pv = s_c;
+    for (int i = wid; i < r; i += nw) {
+      const double *col = A + r0 + (size_t)(r0 + i) * n;
+      double acc = 0.0;
+      for (int j = lane; j < r; j += 32)
+        acc += col[j] * x[j];
+      acc = warp_sum(acc);
+      if (lane == 0)
+        pv[i] = beta * acc;
+    }
+    __syncthreads();
+    double vp = 0.0;
+    for (int i = tid; i < r; i += bd)
+      vp += x[i] * pv[i];
+    vp = blk_allsum(vp, s_red);
+    const double K = 0.5 * beta * vp;
+    for (int i = tid; i < r; i += bd)
+      pv[i] -= K * x[i]; // w = p - K v
+    __syncthreads();
+    // A_sub -= v w^T + w v^T
+    for (int e = tid; e < r * r; e += bd) {
+      const int j = e / r, i = e % r;
+      A[r0 + i + (size_t)(r0 + j) * n] -= x[i] * pv[j] + pv[i] * x[j];
+    }
+    __syncthreads();
+  }
+  if (tid == 0) {
+    if (n >= 2) {
+      s_d[n - 2] = A[(n - 2) + (size_t)(n - 2) * n];
+      s_e[n - 2] = A[(n - 1) + (size_t)(n - 2) * n];
+    }
+    s_d[n - 1] = A[(n - 1) + (size_t)(n - 1) * n];
+    s_e[n - 1] = 0.0;
+    s_fail = 0;
+    double tn = 0.0; // ||T||_inf: the deflation floor eps ||T|| (absolute accuracy)
+    for (int i = 0; i < n; i++)
+      tn = fmax(tn, fabs(s_d[i]) + fabs(s_e[i]) + (i ? fabs(s_e[i - 1]) : 0.0));
+    s_tn = tn;
+  }
+  // ---- 2) Z = H_0 H_1 ... H_{n-3}, accumulated backwards
+  for (int e = tid; e < n * n; e += bd)
+    Z[e] = (e % n == e / n) ? 1.0 : 0.0;
+  __syncthreads();
+  for (int k = n - 3; k >= 0; k--) {
+    const double beta = s_s[k];
+    if (beta == 0.0)
+      continue;
+    const int r0 = k + 1, r = n - r0;
+    const double *v = A + r0 + (size_t)k * n;
+    for (int j = wid; j < r; j += nw) {
+      double *zc = Z + r0 + (size_t)(r0 + j) * n;
+      double acc = 0.0;
+      for (int i = lane; i < r; i += 32)
+        acc += v[i] * zc[i];
+      acc = beta * warp_sum(acc);
+      for (int i = lane; i < r; i += 32)
+        zc[i] -= acc * v[i];
+    }
+    __syncthreads();
+  }
+  // ---- 3) implicit QL on (d, e), rotations applied to the rows of Z
+  for (int l = 0; l < n; l++) {
+    for (int iter = 0;; iter++) {
+      if (tid == 0) {
+        int m = l;
+        for (; m < n - 1; m++) {
+          const double dd = fabs(s_d[m]) + fabs(s_d[m + 1]);
+          if (fabs(s_e[m]) <= 2.2204460492503131e-16 * dd || fabs(s_e[m]) <= 2.2204460492503131e-16 * s_tn)
+            break;
+        }
+        s_m = m;
+        s_lo = m;
+        if (m != l) {
+          if (iter >= 60) {
+            s_fail = 1;
+          } else {
+            double g = (s_d[l + 1] - s_d[l]) / (2.0 * s_e[l]);
+            double r = hypot(g, 1.0);
+            g = s_d[m] - s_d[l] + s_e[l] / (g + copysign(r, g));
+            double sn = 1.0, cs = 1.0, pp = 0.0;
+            int i = m - 1;
+            bool early = false;
+            for (; i >= l; i--) {
+              const double f = sn * s_e[i], b = cs * s_e[i];
+              r = hypot(f, g);
+              s_e[i + 1] = r;
+              if (r == 0.0) {
+                s_d[i + 1] -= pp;
+                s_e[m] = 0.0;
+                early = true;
+                break;
+              }
+              sn = f / r;
+              cs = g / r;
+              g = s_d[i + 1] - pp;
+              r = (s_d[i] - g) * sn + 2.0 * cs * b;
+              pp = sn * r;
+              s_d[i + 1] = g + pp;
+              g = cs * r - b;
+              s_c[i] = cs;
+              s_s[i] = sn;
+            }
+            s_lo = early ? i + 1 : l;
+            if (!early) {
+              s_d[l] -= pp;
+              s_e[l] = g;
+              s_e[m] = 0.0;
+            }
+          }
+        }
+      }
+      __syncthreads();
+      const int m = s_m, lo = s_lo, fl = s_fail;
+      __syncthreads(); // all have read before thread 0 writes the next sweep
+      if (m == l || fl)
+        break;
+      // rotation i mixes columns i and i+1 of every row, for i = m-1 down to lo
+      for (int row = tid; row < n; row += bd) {
+        double xr = Z[row + (size_t)m * n];
+        for (int i = m - 1; i >= lo; i--) {
+          const double zi = Z[row + (size_t)i * n];
+          const double cs = s_c[i], sn = s_s[i];
+          Z[row + (size_t)(i + 1) * n] = sn * zi + cs * xr;
+          xr = cs * zi - sn * xr;
+        }
+        Z[row + (size_t)lo * n] = xr;
+      }
+      __syncthreads();
+    }
+    if (s_fail)
+      break;
+    __syncthreads();
+  }
+  const int fail = s_fail;
+  __syncthreads();
+  if (fail)
+    return 1;
+  // ---- 4) ascending order (ties by index), columns permuted through A
+  for (int i = tid; i < n; i += bd) {
+    const double di = s_d[i];
+    int rank = 0;
+    for (int j = 0; j < n; j++) {
+      const double dj = s_d[j];
+      if (dj < di || (dj == di && j < i))
+        rank++;
+    }
+    ord[rank] = i;
+  }
+  __syncthreads();
+  for (int i = tid; i < n; i += bd)
+    w[i] = s_d[ord[i]];
+  for (int e = tid; e < n * n; e += bd) {
+    const int j = e / n, row = e % n;
+    A[row + (size_t)j * n] = Z[row + (size_t)ord[j] * n];
+  }
+  __syncthreads();
+  for (int e = tid; e < n * n; e += bd)
+    Z[e] = A[e];
+  __syncthreads();
+  return 0;
+}
+
 // In-place Cholesky of the lower triangle of A (n x n, ld n). Returns 0 on
 // success or k+1 when pivot k is <= 0 (NaN pivots pass, like Eigen::LLT).
 KR_DEV int block_cholesky(int n, double *A) {

@@ -242,7 +242,22 @@ template <class Team> struct LobpcgSolver {
       block_lower_inverse(p, d.Sj, d.Li);
       block_gemm_nn(p, d.Li, false, G, false, d.Tm);  // T = Li G
       block_gemm_nn(p, d.Tm, false, d.Li, true, d.Cm); // C = T Li^T
-      block_jacobi_eig(p, d.Cm, d.th, d.Q, d.eig_cs, d.eig_pq, d.eig_ord);
+      // C symmetric to the last bit, then tridiagonal QL on a copy (Jacobi on
+      // C itself if QL does not converge)
+      for (int e = threadIdx.x; e < p * p; e += blockDim.x) {
+        const int j = e / p, i = e % p;
+        if (i > j) {
+          const double c = 0.5 * (d.Cm[e] + d.Cm[j + (size_t)i * p]);
+          d.Cm[e] = c;
+          d.Cm[j + (size_t)i * p] = c;
+        }
+      }
+      __syncthreads();
+      for (int e = threadIdx.x; e < p * p; e += blockDim.x)
+        d.Tm[e] = d.Cm[e];
+      __syncthreads();
+      if (block_sym_eig_ql(p, d.Tm, d.th, d.Q, d.eig_ord) != 0)
+        block_jacobi_eig(p, d.Cm, d.th, d.Q, d.eig_cs, d.eig_pq, d.eig_ord);
       __shared__ int s_fin;
       if (threadIdx.x == 0)
         s_fin = 1;
