@@ -91,6 +91,89 @@ KR_DEV void team_gram2(Team &tm, int64_t n, const double *Z, const double *AZ, i
   tm.sync();
 }
 
+// C = A^T B for tall-skinny A (n x a) and B (n x b), column-major with
+// leading dim ld; C is a x b with leading dim a. DMMA 8x8 tiles, one warp per
+// tile; each block reduces its fixed row range into a private partial, then
+// the partials are summed in block order (deterministic for a team size).
+template <class Team>
+KR_DEV void team_gemm_tn(Team &tm, int64_t n, const double *A, int a, const double *B, int b, int64_t ld,
+                         double *C, double *part) {
+  const int ta = (a + 7) / 8, tb = (b + 7) / 8, ntiles = ta * tb;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int ncta = tm.ncta(), rank = tm.cta_rank();
+  const int64_t per = (n + ncta - 1) / ncta;
+  const int64_t r0 = imin64((int64_t)rank * per, n), r1 = imin64(r0 + per, n);
+  double *my = part + (size_t)rank * a * b;
+  for (int t = wid; t < ntiles; t += nw) {
+    const int bi = t % ta, bj = t / ta;
+    const int ia = bi * 8 + (lane >> 2), jb = bj * 8 + (lane >> 2);
+    const bool va = ia < a, vb = jb < b;
+    const double *pa = A + (int64_t)(va ? ia : 0) * ld;
+    const double *pb = B + (int64_t)(vb ? jb : 0) * ld;
+    double c0 = 0.0, c1 = 0.0, e0 = 0.0, e1 = 0.0;
+    int64_t base = r0;
+    for (; base + 8 <= r1; base += 8) { // two independent accumulators
+      const int64_t r = base + (lane & 3);
+      const double x0 = va ? pa[r] : 0.0, y0 = vb ? pb[r] : 0.0;
+      const double x1 = va ? pa[r + 4] : 0.0, y1 = vb ? pb[r + 4] : 0.0;
+      dmma_8x8x4(c0, c1, x0, y0);
+      dmma_8x8x4(e0, e1, x1, y1);
+    }
+    for (; base < r1; base += 4) {
+      const int64_t r = base + (lane & 3);
+      const bool in = r < r1;
+      const double x0 = (in && va) ? pa[r] : 0.0, y0 = (in && vb) ? pb[r] : 0.0;
+      dmma_8x8x4(c0, c1, x0, y0);
+    }
+    c0 += e0;
+    c1 += e1;
+    const int ci = bi * 8 + (lane >> 2), cj = bj * 8 + 2 * (lane & 3);
+    if (ci < a) {
+      if (cj < b)
+        my[ci + (size_t)cj * a] = c0;
+      if (cj + 1 < b)
+        my[ci + (size_t)(cj + 1) * a] = c1;
+    }
+  }
+  tm.sync();
+  const int64_t nt = tm.nthreads();
+  for (int64_t e = tm.tid(); e < (int64_t)a * b; e += nt) {
+    double s = 0.0;
+    for (int r = 0; r < ncta; r++)
+      s += __ldcg(part + (size_t)r * a * b + e);
+    C[e] = s;
+  }
+  tm.sync();
+}
+
+// X[:, i] -= sum_j S[:, j] * Cc(j, i) for i < k, j < ns (X, S column-major
+// with leading dim ld; Cc leading dim ldc).
+template <class Team>
+KR_DEV void team_combine_sub(Team &tm, int64_t n, const double *S, int64_t ld, int ns, const double *Cc, int ldc,
+                             int k, double *X) {
+  const int64_t nt = tm.nthreads();
+  for (int64_t r = tm.tid(); r < n; r += nt) {
+    for (int i0 = 0; i0 < k; i0 += 8) {
+      double acc[8];
+#pragma unroll
+      for (int t = 0; t < 8; t++)
+        acc[t] = (i0 + t < k) ? X[(int64_t)(i0 + t) * ld + r] : 0.0;
+      for (int j = 0; j < ns; j++) {
+        const double z = S[(int64_t)j * ld + r];
+        const double *cj = Cc + j;
+#pragma unroll
+        for (int t = 0; t < 8; t++)
+          if (i0 + t < k)
+            acc[t] -= __ldg(cj + (size_t)(i0 + t) * ldc) * z;
+      }
+#pragma unroll
+      for (int t = 0; t < 8; t++)
+        if (i0 + t < k)
+          X[(int64_t)(i0 + t) * ld + r] = acc[t];
+    }
+  }
+}
+
 // out[:, i] = sum_j Y(roff + j, i) * Z[:, j], i < q, j < zc (column-major,
 // both with leading dim ld; Y leading dim ldy).
 template <class Team>

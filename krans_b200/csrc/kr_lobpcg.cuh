@@ -154,8 +154,133 @@ template <class Team> struct LobpcgSolver {
       t_ph[3] += globaltimer_ns() - t0;
     return ok;
   }
+  // Block form of orthonormalize_cols_mgs below, same result up to rounding:
+  // (1) every column gets one classical projection against the basis
+  //     (C = B^T X, X -= B C on the tensor cores) and is normalised;
+  // (2) the MGS (with reorthogonalisation) of the block is done as Cholesky
+  //     QR, twice: G = V^T V = L L^T, V <- V L^-T. For full-rank input both
+  //     give the same Q (the QR factor with positive diagonal R), and MGS's
+  //     failure test (a column norm below tol after removing the earlier
+  //     columns) is the test on the Cholesky pivots. When a Cholesky fails
+  //     (dependent columns, or a block too ill-conditioned for Cholesky QR),
+  //     the column-wise path decides on the same input.
   __device__ __noinline__ bool orthonormalize_cols(double *Xb, int64_t k, const double *basis, int64_t nb, double tol,
                                                    bool reorth, double *scratch) {
+    if (k <= 0)
+      return true;
+    if (nb > 0) {
+      team_gemm_tn(tm, n, basis, (int)nb, Xb, (int)k, ldn, d.Cm, d.gram_part);
+      team_combine_sub(tm, n, basis, ldn, (int)nb, d.Cm, (int)nb, (int)k, Xb);
+      tm.sync();
+      gram_flops += 4.0 * (double)n * nb * k;
+      c.bytes += 8.0 * n * (2.0 * nb + 3.0 * k);
+    }
+    if (!normalize_cols(Xb, k, tol))
+      return false;
+    if (cholqr_round(Xb, k, tol, scratch) && (!reorth || cholqr_round(scratch, k, tol, Xb))) {
+      if (!reorth)
+        for (int64_t i = 0; i < k; i++)
+          copy(col(scratch, i), col(Xb, i));
+      return true;
+    }
+    for (int64_t i = 0; i < k; i++)
+      copy(col(Xb, i), col(scratch, i));
+    if (!mgs_cols(scratch, k, tol, reorth))
+      return false;
+    for (int64_t i = 0; i < k; i++)
+      copy(col(scratch, i), col(Xb, i));
+    return true;
+  }
+
+  // scale each of k columns to unit norm; false if a norm is below tol
+  __device__ __noinline__ bool normalize_cols(double *Xb, int64_t k, double tol) {
+    for (int64_t q0 = 0; q0 < k; q0 += KR_RED_K) {
+      const int cnt = (int)imin64(KR_RED_K, k - q0);
+      double acc[KR_RED_K];
+#pragma unroll
+      for (int t = 0; t < KR_RED_K; t++)
+        acc[t] = 0.0;
+      for (int64_t i = tm.tid(); i < n; i += tm.nthreads()) {
+#pragma unroll
+        for (int t = 0; t < KR_RED_K; t++)
+          if (t < cnt) {
+            const double x = Xb[(q0 + t) * ldn + i];
+            acc[t] += x * x;
+          }
+      }
+      tm.template sum<KR_RED_K>(acc);
+      double inv[KR_RED_K];
+      bool bad = false;
+#pragma unroll
+      for (int t = 0; t < KR_RED_K; t++) {
+        const double nr = sqrt(acc[t]);
+        inv[t] = 1.0;
+        if (t < cnt) {
+          if (!(nr >= tol))
+            bad = true;
+          inv[t] = 1.0 / nr;
+        }
+      }
+      if (bad)
+        return false;
+      for (int64_t i = tm.tid(); i < n; i += tm.nthreads()) {
+#pragma unroll
+        for (int t = 0; t < KR_RED_K; t++)
+          if (t < cnt)
+            Xb[(q0 + t) * ldn + i] *= inv[t];
+      }
+      c.bytes += 24.0 * n * cnt;
+    }
+    tm.sync();
+    return true;
+  }
+
+  // d.Tm <- L^-T for the Cholesky factor L of the k x k matrix in d.Sj (lead
+  // block). False if a pivot is not positive or below tol.
+  __device__ __noinline__ bool chol_inv_t(int k, double tol) {
+    if (tm.lead_cta()) {
+      __shared__ int s_bad;
+      const int f = block_cholesky(k, d.Sj);
+      if (threadIdx.x == 0)
+        s_bad = f != 0;
+      __syncthreads();
+      if (!s_bad) {
+        for (int i = threadIdx.x; i < k; i += blockDim.x)
+          if (!(d.Sj[i + (size_t)i * k] >= tol))
+            s_bad = 1;
+        __syncthreads();
+      }
+      if (!s_bad) {
+        block_lower_inverse(k, d.Sj, d.Li);
+        for (int e = threadIdx.x; e < k * k; e += blockDim.x) {
+          const int j = e / k, i = e % k;
+          d.Tm[e] = d.Li[j + (size_t)i * k];
+        }
+        __syncthreads();
+      }
+      if (threadIdx.x == 0)
+        *d.flag = s_bad;
+      __syncthreads();
+    }
+    tm.publish();
+    return *(volatile int32_t *)d.flag == 0;
+  }
+
+  // one Cholesky-QR round: out = V chol(V^T V)^-T (V unchanged)
+  __device__ __noinline__ bool cholqr_round(const double *V, int64_t k, double tol, double *out) {
+    team_gemm_tn(tm, n, V, (int)k, V, (int)k, ldn, d.Sj, d.gram_part);
+    gram_flops += 2.0 * (double)n * k * k;
+    c.bytes += 8.0 * n * k;
+    if (!chol_inv_t((int)k, tol))
+      return false;
+    team_combine(tm, n, V, ldn, (int)k, d.Tm, (int)k, 0, (int)k, out);
+    c.bytes += 16.0 * n * k;
+    tm.sync();
+    return true;
+  }
+
+  __device__ __noinline__ bool orthonormalize_cols_mgs(double *Xb, int64_t k, const double *basis, int64_t nb,
+                                                       double tol, bool reorth, double *scratch) {
     for (int64_t i = 0; i < k; i++) {
       double *xi = col(Xb, i);
       gs_pass(basis, nb, xi);
@@ -190,19 +315,59 @@ template <class Team> struct LobpcgSolver {
     c.bytes += 2.0 * 8.0 * n * p;
   }
 
-  // solve_tiny_gep (LOBPCGSolver.cpp:88-119) on the leader block; theta in
-  // d.th, eigenvectors in d.Ym (ld p). Returns false if S is not SPD.
+  // solve_tiny_gep (LOBPCGSolver.cpp:88-119): symmetrise, Cholesky of S with
+  // the reference's jitter ladder, C = L^-1 G L^-T, eigenpairs of C (theta
+  // ascending in d.th), Y = L^-T Q in d.Ym (ld p). The three p x p products
+  // run on the whole team; the factorisations and the eigensolver run on the
+  // leader block. Returns false if no jitter makes S positive definite (or
+  // the eigenvalues are not finite).
   __device__ __noinline__ bool tiny_gep(int p) {
     const uint64_t t0 = globaltimer_ns();
     if (tm.lead_cta())
-      gep_block(p);
+      gep_prep(p);
     tm.publish();
+    bool ok = false;
+    for (int t = 0; t < 4 && !ok; t++) {
+      if (tm.lead_cta())
+        gep_chol(p, t);
+      tm.publish();
+      const bool chol_ok = *(volatile int32_t *)d.flag == 0;
+      tm.sync(); // every block has read the flag before the leader writes it again
+      if (!chol_ok)
+        continue;
+      team_small_gemm(p, d.Li, false, d.G, false, d.Tm);  // T = L^-1 G
+      team_small_gemm(p, d.Tm, false, d.Li, true, d.Cm); // C = T L^-T
+      if (tm.lead_cta())
+        gep_eig(p);
+      tm.publish();
+      const bool eig_ok = *(volatile int32_t *)d.flag == 0;
+      tm.sync();
+      if (!eig_ok)
+        continue;
+      team_small_gemm(p, d.Li, true, d.Q, false, d.Ym); // Y = L^-T Q
+      ok = true;
+    }
     t_ph[2] += globaltimer_ns() - t0;
-    return *(volatile int32_t *)d.flag == 0;
+    return ok;
   }
-  __device__ __noinline__ void gep_block(int p) {
+  // C = op(A) op(B) for p x p matrices (ld p) on the whole team
+  KR_DEV void team_small_gemm(int p, const double *A, bool ta, const double *B, bool tb, double *C) {
+    const int64_t nt = tm.nthreads();
+    for (int64_t e = tm.tid(); e < (int64_t)p * p; e += nt) {
+      const int j = (int)(e / p), i = (int)(e % p);
+      double s = 0.0;
+      for (int q = 0; q < p; q++) {
+        const double x = ta ? A[q + (size_t)i * p] : A[i + (size_t)q * p];
+        const double y = tb ? B[j + (size_t)q * p] : B[q + (size_t)j * p];
+        s += x * y;
+      }
+      C[e] = s;
+    }
+    tm.sync();
+  }
+  // leader block: symmetrise S and G; ||S||_F (floored at 1) into d.dflag[0]
+  __device__ __noinline__ void gep_prep(int p) {
     double *S = d.S, *G = d.G;
-    // symmetrize
     for (int e = threadIdx.x; e < p * p; e += blockDim.x) {
       const int j = e / p, i = e % p;
       if (i >= j) {
@@ -215,64 +380,63 @@ template <class Team> struct LobpcgSolver {
       }
     }
     __syncthreads();
-    __shared__ double s_norm;
-    {
-      double s = 0.0;
-      for (int e = threadIdx.x; e < p * p; e += blockDim.x)
-        s += S[e] * S[e];
-      int b = 0;
-      double v[1] = {s};
-      block_sum<1>(tm.sh, b, v);
-      if (threadIdx.x == 0)
-        s_norm = fmax(1.0, sqrt(v[0]));
-      __syncthreads();
-    }
-    const double jit[4] = {0.0, 1e-14, 1e-12, 1e-10};
-    int ok = 0;
-    for (int t = 0; t < 4 && !ok; t++) {
-      for (int e = threadIdx.x; e < p * p; e += blockDim.x) {
-        double v = S[e];
-        if (jit[t] > 0.0 && (e % p) == (e / p))
-          v += jit[t] * s_norm;
-        d.Sj[e] = v;
-      }
-      __syncthreads();
-      if (block_cholesky(p, d.Sj) != 0)
-        continue;
-      block_lower_inverse(p, d.Sj, d.Li);
-      block_gemm_nn(p, d.Li, false, G, false, d.Tm);  // T = Li G
-      block_gemm_nn(p, d.Tm, false, d.Li, true, d.Cm); // C = T Li^T
-      // C symmetric to the last bit, then tridiagonal QL on a copy (Jacobi on
-      // C itself if QL does not converge)
-      for (int e = threadIdx.x; e < p * p; e += blockDim.x) {
-        const int j = e / p, i = e % p;
-        if (i > j) {
-          const double c = 0.5 * (d.Cm[e] + d.Cm[j + (size_t)i * p]);
-          d.Cm[e] = c;
-          d.Cm[j + (size_t)i * p] = c;
-        }
-      }
-      __syncthreads();
-      for (int e = threadIdx.x; e < p * p; e += blockDim.x)
-        d.Tm[e] = d.Cm[e];
-      __syncthreads();
-      if (block_sym_eig_ql(p, d.Tm, d.th, d.Q, d.eig_ord) != 0)
-        block_jacobi_eig(p, d.Cm, d.th, d.Q, d.eig_cs, d.eig_pq, d.eig_ord);
-      __shared__ int s_fin;
-      if (threadIdx.x == 0)
-        s_fin = 1;
-      __syncthreads();
-      for (int i = threadIdx.x; i < p; i += blockDim.x)
-        if (!isfinite(d.th[i]))
-          s_fin = 0;
-      __syncthreads();
-      if (!s_fin)
-        continue;
-      block_gemm_nn(p, d.Li, true, d.Q, false, d.Ym); // Y = Li^T Q
-      ok = 1;
-    }
+    double s = 0.0;
+    for (int e = threadIdx.x; e < p * p; e += blockDim.x)
+      s += S[e] * S[e];
+    int b = 0;
+    double v[1] = {s};
+    block_sum<1>(tm.sh, b, v);
     if (threadIdx.x == 0)
-      *d.flag = ok ? 0 : 1;
+      d.dflag[0] = fmax(1.0, sqrt(v[0]));
+    __syncthreads();
+  }
+  // leader block: Cholesky of S + jitter_t ||S|| I and L^-1 into d.Li;
+  // d.flag = 0 on success
+  __device__ __noinline__ void gep_chol(int p, int t) {
+    const double jit[4] = {0.0, 1e-14, 1e-12, 1e-10};
+    const double sn = *(volatile double *)d.dflag;
+    for (int e = threadIdx.x; e < p * p; e += blockDim.x) {
+      double v = d.S[e];
+      if (jit[t] > 0.0 && (e % p) == (e / p))
+        v += jit[t] * sn;
+      d.Sj[e] = v;
+    }
+    __syncthreads();
+    const int f = block_cholesky(p, d.Sj);
+    if (f == 0)
+      block_lower_inverse(p, d.Sj, d.Li);
+    if (threadIdx.x == 0)
+      *d.flag = f != 0;
+    __syncthreads();
+  }
+  // leader block: eigenpairs of C (made exactly symmetric): tridiagonal QL on
+  // a copy, Jacobi on C itself if QL does not converge; d.flag = 0 when all
+  // eigenvalues are finite
+  __device__ __noinline__ void gep_eig(int p) {
+    for (int e = threadIdx.x; e < p * p; e += blockDim.x) {
+      const int j = e / p, i = e % p;
+      if (i > j) {
+        const double c = 0.5 * (d.Cm[e] + d.Cm[j + (size_t)i * p]);
+        d.Cm[e] = c;
+        d.Cm[j + (size_t)i * p] = c;
+      }
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < p * p; e += blockDim.x)
+      d.Tm[e] = d.Cm[e];
+    __syncthreads();
+    if (block_sym_eig_ql(p, d.Tm, d.th, d.Q, d.eig_ord) != 0)
+      block_jacobi_eig(p, d.Cm, d.th, d.Q, d.eig_cs, d.eig_pq, d.eig_ord);
+    __shared__ int s_bad;
+    if (threadIdx.x == 0)
+      s_bad = 0;
+    __syncthreads();
+    for (int i = threadIdx.x; i < p; i += blockDim.x)
+      if (!isfinite(d.th[i]))
+        s_bad = 1;
+    __syncthreads();
+    if (threadIdx.x == 0)
+      *d.flag = s_bad;
     __syncthreads();
   }
 
