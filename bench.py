@@ -409,7 +409,7 @@ def run_quickstart(args):
     ctx = kb.Context(0)
     inst = G.shift_operator(1000, 3, 0.5)
     A = inst.A
-    cyc, lob, e2e, dists = [], [], [], []
+    cyc, lob, e2e, dists, ph_c, ph_l = [], [], [], [], [], []
 
     def loop():
         for it in range(args.warmup + args.steps):
@@ -422,6 +422,8 @@ def run_quickstart(args):
             Ul = kb.basis_to_numpy(Rl.right_null)
             t1 = time.perf_counter()
             if it >= args.warmup:
+                ph_c.append(Rc.phase_ms)
+                ph_l.append(Rl.phase_ms)
                 cyc.append(Rc.device_ms * 1e3)
                 lob.append(Rl.device_ms * 1e3)
                 e2e.append((t1 - t0) * 1e6)
@@ -449,6 +451,8 @@ def run_quickstart(args):
         "config": {"workload": "shift operator n=1000, N=3, c=0.5 (the reference's quickstart), k=3",
                    "l2": "resident (44 KB problem; latency-bound)"},
         "cyclic_us": med(cyc), "lobpcg_us": med(lob), "max_subspace_dist": max(dists),
+        "cyclic_phase_ms": dict(zip(["lanczos", "tiny_svd", "cg_polish", "rest"], ph_c[-1])),
+        "lobpcg_phase_ms": dict(zip(["apply_normal", "gram", "tiny_gep", "orthonormalise", "rest"], ph_l[-1])),
         "e2e": {"value": med(e2e), "unit": "us",
                 "h2d_bytes_per_step": int(A.data.nbytes + A.indices.nbytes + A.indptr.nbytes),
                 "d2h_bytes_per_step": 6 * 1000 * 8},

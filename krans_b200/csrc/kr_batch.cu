@@ -40,6 +40,7 @@ struct BatchLaunch {
   int precision = 0;
   int grid = 0;        // CTA-team blocks (small requests)
   int n_large = 0;     // requests [0, n_large) run on clusters
+  size_t dyn_smem = 0; // dynamic shared memory per block (CG vectors of one-block solves)
   int csize = 8;       // blocks per cluster
   int nclusters = 0;   // resident clusters of the cluster launch
   size_t stride_L = 0; // workspace slot of one cluster
@@ -141,13 +142,21 @@ struct BatchLaunch {
     stride_L = (size_t)kr_round_up((int64_t)std::max<size_t>(stride_L, 256), 256);
     const int n_small = n - n_large;
     const bool mixed = precision == KRANS_PREC_MIXED;
+    // dynamic shared memory for the CG vectors of one-block solves: the
+    // largest small request that fits under the cap
+    dyn_smem = 0;
+    for (int pos = n_large; pos < n; pos++) {
+      const size_t b = cta_cg_smem_bytes(hreq[pos].plan.ldm, hreq[pos].plan.ldn);
+      if (b <= cta_smem_cap())
+        dyn_smem = std::max(dyn_smem, b);
+    }
     const int per_sm = cyclic_batch_cta_per_sm(mixed);
     grid = n_small > 0 ? std::max(1, std::min(n_small, ctx->sms * per_sm)) : 0;
     nclusters = 0;
     if (n_large > 0) {
       // one cluster launch fills the GPU; its blocks take the small requests
       // after the large queue is empty (one small-request slot per block)
-      const int maxc = cyclic_batch_cluster_max(mixed, csize, ctx->sms);
+      const int maxc = cyclic_batch_cluster_max(mixed, csize, ctx->sms, dyn_smem);
       nclusters = std::max(1, maxc);
       grid = nclusters * csize;
     }
@@ -211,10 +220,11 @@ struct BatchLaunch {
     const bool mixed = precision == KRANS_PREC_MIXED;
     if (e == cudaSuccess) {
       if (n_large > 0)
-        e = launch_cyclic_batch_cluster(mixed, nclusters, csize, s, d_reqs, n_large, d_queue, ws_large, stride_L,
+        e = launch_cyclic_batch_cluster(mixed, nclusters, csize, dyn_smem, s, d_reqs, n_large, d_queue, ws_large,
+                                        stride_L,
                                         d_reqs + n_large, count - n_large, d_queue + 1, ws_small, ws_stride);
       else
-        e = launch_cyclic_batch_cta(mixed, grid, s, d_reqs, count, d_queue + 1, ws_small, ws_stride);
+        e = launch_cyclic_batch_cta(mixed, grid, 512, dyn_smem, s, d_reqs, count, d_queue + 1, ws_small, ws_stride);
     }
     if (e == cudaSuccess)
       e = cudaEventRecord(ev1, s);

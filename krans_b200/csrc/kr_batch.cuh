@@ -24,6 +24,8 @@ template <class Team> KR_DEV double team_max_residual(Team &tm, const CsrView &F
   return mr;
 }
 
+extern __shared__ __align__(16) char kr_dyn_smem[];
+
 // One request on one thread block, with its workspace laid out in `slot`.
 template <class KT>
 __device__ __noinline__ void run_cta_request(TeamShared *sh, CyclicDesc *dp, const CyclicRequestDev &rq,
@@ -44,6 +46,15 @@ __device__ __noinline__ void run_cta_request(TeamShared *sh, CyclicDesc *dp, con
     d.ldb = rq.plan.ldb;
     d.status = rq.status;
     d.res = rq.res;
+    // CG vectors in dynamic shared memory when the launch gave enough of it
+    // (the solver reaches them through generic pointers)
+    uint32_t dyn;
+    asm volatile("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn));
+    if (cta_cg_smem_bytes(rq.plan.ldm, rq.plan.ldn) <= (size_t)dyn) {
+      d.rp = reinterpret_cast<double2 *>(kr_dyn_smem);
+      d.Ap = reinterpret_cast<double *>(kr_dyn_smem + 16 * rq.plan.ldm);
+      d.tn = reinterpret_cast<double *>(kr_dyn_smem + 24 * rq.plan.ldm);
+    }
     rq.res->t_begin = globaltimer_ns();
   }
   __syncthreads();

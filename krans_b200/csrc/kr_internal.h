@@ -12,6 +12,21 @@
 
 #include "../../include/krans_cuda.h"
 
+#include <cstdlib>
+
+// Cap on the dynamic shared memory a one-block solve uses for its CG vectors
+// (KRANS_SMEM_CG_KB, default 0: global memory). Measured on B200: 160 KiB
+// gave 8% less CG time on a 1000-unknown solve and cost 16% of a batch of
+// uneven solves, whose cluster teams lose L1 capacity to the carve-out. Larger
+// carve-outs leave less of the SM's 256 KiB to the L1 cache.
+inline size_t cta_smem_cap() {
+  static const size_t cap = [] {
+    const char *e = getenv("KRANS_SMEM_CG_KB");
+    return (size_t)(e ? atoll(e) : 0) * 1024;
+  }();
+  return cap;
+}
+
 namespace kr {
 
 void set_error(const char *fmt, ...);

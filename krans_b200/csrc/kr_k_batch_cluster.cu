@@ -10,10 +10,12 @@ static const void *cl_kernel(bool mixed) {
   return mixed ? (const void *)cyclic_batch_cluster_kernel<float> : (const void *)cyclic_batch_cluster_kernel<double>;
 }
 
-static cudaLaunchConfig_t cl_config(int nclusters, int csize, cudaStream_t s, cudaLaunchAttribute *at) {
+static cudaLaunchConfig_t cl_config(int nclusters, int csize, size_t dyn_smem, cudaStream_t s,
+                                    cudaLaunchAttribute *at) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(nclusters * csize);
   cfg.blockDim = dim3(512);
+  cfg.dynamicSmemBytes = dyn_smem;
   cfg.stream = s;
   at[0].id = cudaLaunchAttributeClusterDimension;
   at[0].val.clusterDim.x = csize;
@@ -24,11 +26,12 @@ static cudaLaunchConfig_t cl_config(int nclusters, int csize, cudaStream_t s, cu
   return cfg;
 }
 
-int cyclic_batch_cluster_max(bool mixed, int csize, int sms) {
+int cyclic_batch_cluster_max(bool mixed, int csize, int sms, size_t dyn_smem) {
   if (csize > 8)
     cudaFuncSetAttribute(cl_kernel(mixed), cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+  cudaFuncSetAttribute(cl_kernel(mixed), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn_smem);
   cudaLaunchAttribute at[1];
-  cudaLaunchConfig_t cfg = cl_config(64, csize, nullptr, at);
+  cudaLaunchConfig_t cfg = cl_config(64, csize, dyn_smem, nullptr, at);
   int maxc = 0;
   if (cudaOccupancyMaxActiveClusters(&maxc, cl_kernel(mixed), &cfg) != cudaSuccess || maxc < 1) {
     cudaGetLastError();
@@ -37,12 +40,15 @@ int cyclic_batch_cluster_max(bool mixed, int csize, int sms) {
   return maxc;
 }
 
-cudaError_t launch_cyclic_batch_cluster(bool mixed, int nclusters, int csize, cudaStream_t s,
+cudaError_t launch_cyclic_batch_cluster(bool mixed, int nclusters, int csize, size_t dyn_smem, cudaStream_t s,
                                         const CyclicRequestDev *reqs_large, int n_large, int *queue_large,
                                         char *ws_large, size_t stride_large, const CyclicRequestDev *reqs_small,
                                         int n_small, int *queue_small, char *ws_small, size_t stride_small) {
   cudaLaunchAttribute at[1];
-  cudaLaunchConfig_t cfg = cl_config(nclusters, csize, s, at);
+  cudaError_t e = cudaFuncSetAttribute(cl_kernel(mixed), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn_smem);
+  if (e != cudaSuccess)
+    return e;
+  cudaLaunchConfig_t cfg = cl_config(nclusters, csize, dyn_smem, s, at);
   if (mixed)
     return cudaLaunchKernelEx(&cfg, cyclic_batch_cluster_kernel<float>, reqs_large, n_large, queue_large, ws_large,
                               stride_large, reqs_small, n_small, queue_small, ws_small, stride_small);

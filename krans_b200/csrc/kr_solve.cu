@@ -155,7 +155,11 @@ static int run_cyclic(krans_ctx *ctx, const krans_mat *A, bool trans, krans_rng 
     e = cudaEventRecord(e0, s);
   if (e == cudaSuccess)
     e = grid ? launch_cyclic_grid(mixed, d, p.grid_blocks, threads, s)
-             : launch_cyclic_batch_cta(mixed, 1, s, d_req, 1, d_queue, slot, 0);
+             : launch_cyclic_batch_cta(mixed, 1, threads,
+                                       cta_cg_smem_bytes(p.ldm, p.ldn) <= cta_smem_cap()
+                                           ? cta_cg_smem_bytes(p.ldm, p.ldn)
+                                           : 0,
+                                       s, d_req, 1, d_queue, slot, 0);
   if (e == cudaSuccess)
     e = cudaEventRecord(e1, s);
   if (e == cudaSuccess)

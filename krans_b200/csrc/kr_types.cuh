@@ -93,6 +93,12 @@ struct CyclicPlan {
 
 __host__ __device__ inline int64_t kr_round_up(int64_t x, int64_t a) { return (x + a - 1) / a * a; }
 
+// Shared-memory bytes that hold the CG vectors of a one-block solve (residual
+// and direction interleaved, F F^T p, F^T p): 16 ldm + 8 ldm + 8 ldn.
+__host__ __device__ inline size_t cta_cg_smem_bytes(int64_t ldm, int64_t ldn) {
+  return (size_t)(24 * ldm + 8 * ldn);
+}
+
 struct Carver {
   size_t off = 0;
   char *base = nullptr;
@@ -222,10 +228,10 @@ struct LobpcgDesc {
 int cyclic_grid_blocks(krans_ctx *ctx, bool mixed, int threads);
 cudaError_t launch_cyclic_grid(bool mixed, const CyclicDesc &d, int blocks, int threads, cudaStream_t s);
 int cyclic_batch_cta_per_sm(bool mixed);
-cudaError_t launch_cyclic_batch_cta(bool mixed, int grid, cudaStream_t s, const CyclicRequestDev *reqs, int count,
+cudaError_t launch_cyclic_batch_cta(bool mixed, int grid, int block, size_t dyn_smem, cudaStream_t s, const CyclicRequestDev *reqs, int count,
                                     int *queue, char *ws, size_t stride);
-int cyclic_batch_cluster_max(bool mixed, int csize, int sms);
-cudaError_t launch_cyclic_batch_cluster(bool mixed, int nclusters, int csize, cudaStream_t s,
+int cyclic_batch_cluster_max(bool mixed, int csize, int sms, size_t dyn_smem);
+cudaError_t launch_cyclic_batch_cluster(bool mixed, int nclusters, int csize, size_t dyn_smem, cudaStream_t s,
                                         const CyclicRequestDev *reqs_large, int n_large, int *queue_large,
                                         char *ws_large, size_t stride_large, const CyclicRequestDev *reqs_small,
                                         int n_small, int *queue_small, char *ws_small, size_t stride_small);

@@ -116,3 +116,29 @@ def test_mixed_precision_reaches_fp64_accuracy(ctx, oracle, team):
     assert U.shape[0] == inst.k and R.converged_to_target
     assert max(np.linalg.norm(A @ u) for u in U) / normA <= 1e-12
     assert oracle.subspace_dist(inst.kernel, U) <= 1e-10
+
+
+def test_shared_memory_cg_vectors_same_answers():
+    """KRANS_SMEM_CG_KB puts the CG vectors of one-block solves in shared
+    memory (read once per process, so checked in a child process)."""
+    import os
+    import subprocess
+    import sys
+    code = (
+        "import numpy as np, krans_b200 as kb\n"
+        "from krans_b200 import generators as G\n"
+        "ctx = kb.Context(0)\n"
+        "inst = G.shift_operator(1000, 3, 0.5)\n"
+        "M = kb.CudaCsrMatrixAdapter.from_scipy(ctx, inst.A)\n"
+        "R = kb.find_nullspace_cyclic_lanczos_ex(M, kb.CudaVectorFactory(ctx, 1000, seed=42),"
+        " kb.CyclicLanczosOptions(k=3, team=1))\n"
+        "U = kb.basis_to_numpy(R.right_null)\n"
+        "P = inst.kernel.T @ np.linalg.lstsq(inst.kernel.T, U.T, rcond=None)[0]\n"
+        "print(U.shape[0], max(np.linalg.norm(inst.A @ u) for u in U), np.linalg.norm(P - U.T, 2))\n")
+    env = dict(os.environ, KRANS_SMEM_CG_KB="160")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = subprocess.run([sys.executable, "-c", code], env=env, cwd=root, capture_output=True, text=True,
+                         timeout=300)
+    assert out.returncode == 0, out.stderr[-2000:]
+    k, res, dist = out.stdout.split()[-3:]
+    assert int(k) == 3 and float(res) < 1e-13 and float(dist) < 1e-10
