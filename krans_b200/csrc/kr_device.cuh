@@ -228,27 +228,24 @@ struct TeamCluster {
     }
     cooperative_groups::cluster_group cl = cooperative_groups::this_cluster();
     cl.sync();
-    if (threadIdx.x < 32) {
-      const unsigned lane = threadIdx.x;
-      double mine[K];
-      const double *peer = cl.map_shared_rank(&sh->cpart[cbuf][0], lane < csize ? lane : 0);
-#pragma unroll
-      for (int k = 0; k < K; k++)
-        mine[k] = lane < csize ? peer[k] : 0.0;
-#pragma unroll
-      for (int k = 0; k < K; k++) {
-        double t = 0.0;
-        for (unsigned r = 0; r < csize; r++)
-          t += __shfl_sync(0xffffffffu, mine[k], r);
-        if (lane == 0)
-          sh->bc[k] = t;
-      }
-    }
-    __syncthreads();
+    // every thread sums the ranks' partials in rank order straight from their
+    // shared memory (the same order as a sequential sum from rank 0). The
+    // next reduction writes the other buffer, and the one after it is behind
+    // that reduction's cluster barrier, which no block passes before all
+    // blocks have read this one.
+    double t[K];
 #pragma unroll
     for (int k = 0; k < K; k++)
-      v[k] = sh->bc[k];
-    __syncthreads();
+      t[k] = 0.0;
+    for (unsigned r = 0; r < csize; r++) {
+      const double *peer = cl.map_shared_rank(&sh->cpart[cbuf][0], r);
+#pragma unroll
+      for (int k = 0; k < K; k++)
+        t[k] += peer[k];
+    }
+#pragma unroll
+    for (int k = 0; k < K; k++)
+      v[k] = t[k];
     cbuf ^= 1;
   }
   KR_DEV double sum1(double x) {
