@@ -73,6 +73,27 @@ int krans_csr_create(krans_ctx *ctx, int64_t m, int64_t n, int64_t nnz,
                      const int32_t *row_ptr, const int32_t *col_idx,
                      const double *values, int flags, krans_mat **out);
 int krans_csr_destroy(krans_mat *A);
+
+/* ---- Matrix files (src/IO/MatrixLoader.cpp:12-56 in the reference:
+ * load_matrix_market, load_ija_triplet_matrix). KRANS_FMT_AUTO picks the format
+ * from the extension (.mtx / .ija), as the reference CLI does
+ * (apps/krans_nullspace.cpp, "Unsupported input format"). IJA: header
+ * "rows cols nnz", then 0-based "i j v" triplets up to the first incomplete
+ * one (a count mismatch only warns on stderr). Matrix Market: coordinate
+ * real/integer/pattern, general/symmetric/skew-symmetric (mirrored), 1-based.
+ * Duplicates are summed; columns are sorted within each row. A file that
+ * cannot be opened or parsed is KRANS_ERR_RUNTIME (std::runtime_error);
+ * an entry outside the stated size is KRANS_ERR_INVALID_ARGUMENT. */
+#define KRANS_FMT_AUTO 0
+#define KRANS_FMT_MTX 1
+#define KRANS_FMT_IJA 2
+/* Parse on the host only: CSR arrays allocated by the library, released
+ * with krans_host_free. */
+int krans_csr_read_host(const char *path, int format, int64_t *m, int64_t *n, int64_t *nnz,
+                        int32_t **row_ptr, int32_t **col_idx, double **values);
+void krans_host_free(void *p);
+/* Parse and create the device matrix (flags as krans_csr_create). */
+int krans_csr_load(krans_ctx *ctx, const char *path, int format, int flags, krans_mat **out);
 int krans_csr_dims(const krans_mat *A, int64_t *m, int64_t *n, int64_t *nnz);
 /* Device pointers of the stored arrays (trans=1: the explicit transpose). */
 int krans_csr_device_arrays(const krans_mat *A, int trans, const int32_t **row_ptr,

@@ -11,7 +11,7 @@ from .api import (  # noqa: F401
     CyclicLanczosOptions, CyclicLanczosResult, LOBPCGOptions, LOBPCGResult,
     Precision, ReorthMode, basis_to_numpy, default_context,
     find_nullspace_cyclic_lanczos, find_nullspace_cyclic_lanczos_ex,
-    find_nullspace_lobpcg, find_nullspace_lobpcg_ex,
+    find_nullspace_lobpcg, find_nullspace_lobpcg_ex, read_matrix,
 )
 
 __all__ = [
@@ -19,5 +19,5 @@ __all__ = [
     "CyclicLanczosOptions", "CyclicLanczosResult", "LOBPCGOptions", "LOBPCGResult",
     "Precision", "ReorthMode", "KransError", "KransInvalidArgument", "basis_to_numpy",
     "default_context", "find_nullspace_cyclic_lanczos", "find_nullspace_cyclic_lanczos_ex",
-    "find_nullspace_lobpcg", "find_nullspace_lobpcg_ex",
+    "find_nullspace_lobpcg", "find_nullspace_lobpcg_ex", "read_matrix",
 ]

@@ -22,6 +22,9 @@ KRANS_RNG_MT19937 = 0
 KRANS_RNG_PHILOX = 1
 KRANS_PREC_FP64 = 0
 KRANS_PREC_MIXED = 1
+KRANS_FMT_AUTO = 0
+KRANS_FMT_MTX = 1
+KRANS_FMT_IJA = 2
 KRANS_TEAM_AUTO = 0
 KRANS_TEAM_CTA = 1
 KRANS_TEAM_GRID = 2
@@ -114,6 +117,11 @@ SIGNATURES = {
     "krans_ctx_sm_count": [P, C.POINTER(I)],
     "krans_csr_create": [P, I64, I64, I64, P, P, P, I, PP],
     "krans_csr_destroy": [P],
+    "krans_csr_read_host": [C.c_char_p, I, C.POINTER(I64), C.POINTER(I64), C.POINTER(I64),
+                            C.POINTER(C.POINTER(C.c_int32)), C.POINTER(C.POINTER(C.c_int32)),
+                            C.POINTER(C.POINTER(C.c_double))],
+    "krans_host_free": [P],
+    "krans_csr_load": [P, C.c_char_p, I, I, PP],
     "krans_csr_dims": [P, C.POINTER(I64), C.POINTER(I64), C.POINTER(I64)],
     "krans_csr_device_arrays": [P, I, PP, PP, PP, PP],
     "krans_vec_create": [P, I64, PP],
@@ -151,7 +159,7 @@ SIGNATURES = {
     "krans_cancel": [P, C.c_uint64],
     "krans_server_drain": [P, D],
 }
-_RESTYPE = {"krans_last_error": C.c_char_p, "krans_version": C.c_char_p}
+_RESTYPE = {"krans_last_error": C.c_char_p, "krans_version": C.c_char_p, "krans_host_free": None}
 
 _lib = None
 

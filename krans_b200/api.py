@@ -16,6 +16,7 @@ from __future__ import annotations
 
 import ctypes as C
 import enum
+import os
 from dataclasses import dataclass, field
 from typing import List, Optional, Sequence
 
@@ -182,6 +183,22 @@ class CudaCsrMatrixAdapter:
         self.h = h
         self.m, self.n, self.nnz = int(m), int(n), nnz
         self.fp32 = fp32
+
+    @classmethod
+    def load(cls, ctx: Context, path: str, fmt: int = K.KRANS_FMT_AUTO, fp32: bool = False) -> "CudaCsrMatrixAdapter":
+        """A .mtx / .ija file (load_matrix_market / load_ija_triplet_matrix,
+        src/IO/MatrixLoader.cpp:12-56) straight into a device matrix."""
+        flags = K.KRANS_CSR_FP64 | (K.KRANS_CSR_FP32 if fp32 else 0)
+        h = C.c_void_p()
+        check(ctx.lib.krans_csr_load(ctx.h, os.fsencode(path), fmt, flags, C.byref(h)), "krans_csr_load")
+        self = cls.__new__(cls)
+        self.ctx = ctx
+        self.h = h
+        m, n, z = C.c_int64(), C.c_int64(), C.c_int64()
+        check(ctx.lib.krans_csr_dims(h, C.byref(m), C.byref(n), C.byref(z)), "krans_csr_dims")
+        self.m, self.n, self.nnz = m.value, n.value, z.value
+        self.fp32 = fp32
+        return self
 
     @classmethod
     def from_scipy(cls, ctx: Context, A, fp32: bool = False) -> "CudaCsrMatrixAdapter":
@@ -457,6 +474,27 @@ def find_nullspace_lobpcg_ex(A: CudaCsrMatrixAdapter, vf: CudaVectorFactory,
 
 def find_nullspace_lobpcg(A, vf, opt) -> List[CudaVectorAdapter]:
     return find_nullspace_lobpcg_ex(A, vf, opt).right_null
+
+
+def read_matrix(path: str, fmt: int = K.KRANS_FMT_AUTO):
+    """Parse a .mtx / .ija file on the host (no GPU): scipy CSR matrix with the
+    reference loader's rules (duplicates summed)."""
+    import scipy.sparse as sp
+    lib = load()
+    m, n, z = C.c_int64(), C.c_int64(), C.c_int64()
+    rp, ci, va = C.POINTER(C.c_int32)(), C.POINTER(C.c_int32)(), C.POINTER(C.c_double)()
+    check(lib.krans_csr_read_host(os.fsencode(path), fmt, C.byref(m), C.byref(n), C.byref(z), C.byref(rp),
+                                  C.byref(ci), C.byref(va)), "krans_csr_read_host")
+    try:
+        M, N, Z = m.value, n.value, z.value
+        indptr = np.ctypeslib.as_array(rp, shape=(M + 1,)).copy()
+        indices = np.ctypeslib.as_array(ci, shape=(max(Z, 1),))[:Z].copy()
+        data = np.ctypeslib.as_array(va, shape=(max(Z, 1),))[:Z].copy()
+    finally:
+        lib.krans_host_free(C.cast(rp, C.c_void_p))
+        lib.krans_host_free(C.cast(ci, C.c_void_p))
+        lib.krans_host_free(C.cast(va, C.c_void_p))
+    return sp.csr_matrix((data, indices, indptr), shape=(M, N))
 
 
 def basis_to_numpy(vs: Sequence[CudaVectorAdapter]) -> np.ndarray:
