@@ -5,6 +5,8 @@
 // include/krans/adapters/eigen/EigenSparseMatrixAdapter.hpp:20-57); like it,
 // vectors of another backend are rejected with std::invalid_argument.
 #include <cstdint>
+#include <memory>
+#include <string>
 #include <vector>
 
 #include "krans/MatrixInterface.hpp"
@@ -28,6 +30,20 @@ public:
     check(krans_csr_create(ctx, (int64_t)m, (int64_t)n, nnz, row_ptr.data(), col_idx.data(), values.data(),
                            KRANS_CSR_FP64 | (fp32 ? KRANS_CSR_FP32 : 0), &A_),
           "krans_csr_create");
+  }
+  /** adopt a matrix created through the C ABI (e.g. krans_csr_load) */
+  CudaCsrMatrixAdapter(krans_ctx *ctx, krans_mat *adopt) : ctx_(ctx), A_(adopt) {
+    int64_t m = 0, n = 0, nnz = 0;
+    check(krans_csr_dims(adopt, &m, &n, &nnz), "krans_csr_dims");
+    m_ = (std::size_t)m;
+    n_ = (std::size_t)n;
+  }
+  /** load a .mtx / .ija file straight into device memory */
+  static std::unique_ptr<CudaCsrMatrixAdapter> load(krans_ctx *ctx, const std::string &path, bool fp32 = false) {
+    krans_mat *A = nullptr;
+    check(krans_csr_load(ctx, path.c_str(), KRANS_FMT_AUTO, KRANS_CSR_FP64 | (fp32 ? KRANS_CSR_FP32 : 0), &A),
+          "krans_csr_load");
+    return std::unique_ptr<CudaCsrMatrixAdapter>(new CudaCsrMatrixAdapter(ctx, A));
   }
   ~CudaCsrMatrixAdapter() override { krans_csr_destroy(A_); }
   CudaCsrMatrixAdapter(const CudaCsrMatrixAdapter &) = delete;

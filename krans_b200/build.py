@@ -29,11 +29,14 @@ def _sources():
 
 def _deps():
     return _sources() + sorted(glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.h"))
-                               + glob.glob(os.path.join(HERE, "..", "include", "*.h")))
+                               + glob.glob(os.path.join(HERE, "..", "include", "*.h"))
+                               + glob.glob(os.path.join(HERE, "..", "include", "krans", "**", "*.hpp"),
+                                           recursive=True)
+                               + [os.path.join(HERE, "cli", "krans_nullspace.cpp")])
 
 
 def up_to_date() -> bool:
-    if not os.path.exists(LIB):
+    if not os.path.exists(LIB) or not os.path.exists(os.path.join(os.path.dirname(LIB), "krans_nullspace")):
         return False
     t = os.path.getmtime(LIB)
     return all(os.path.getmtime(p) <= t for p in _deps())
@@ -65,7 +68,22 @@ def build(force: bool = False, verbose: bool = False) -> str:
     tmp = LIB + ".tmp"
     subprocess.run([NVCC, *ARCH, "-shared", "--cudart", "static", "-o", tmp, *objs], check=True)
     os.replace(tmp, LIB)
+    build_cli()
     return LIB
+
+
+CLI_SRC = os.path.join(HERE, "cli", "krans_nullspace.cpp")
+CLI = os.path.join(os.path.dirname(LIB), "krans_nullspace")
+
+
+def build_cli() -> str:
+    """The command-line tool (C++ over the drop-in headers and the library)."""
+    libdir = os.path.dirname(LIB)
+    tmp = CLI + ".tmp"
+    subprocess.run(["g++", "-std=c++17", "-O2", "-I", os.path.join(HERE, "..", "include"), CLI_SRC, "-o", tmp,
+                    "-L", libdir, "-l:" + os.path.basename(LIB), "-Wl,-rpath,$ORIGIN"], check=True)
+    os.replace(tmp, CLI)
+    return CLI
 
 
 if __name__ == "__main__":
