@@ -51,6 +51,8 @@ struct CyclicLanczosOptions {
   int precision = KRANS_PREC_FP64; // KRANS_PREC_MIXED: FP32 SpMV/Lanczos, FP64 reorth/SVD/polish
   int team = KRANS_TEAM_AUTO;
   int polish_block = 0; // 1: project up to 8 candidates per restart with one block CG
+  int precond_device = KRANS_PRECOND_NONE; // device form of precond_AAt (KRANS_PRECOND_JACOBI / _SD)
+  int precond_steps = 8;
 };
 
 struct CyclicLanczosResult {
@@ -72,7 +74,8 @@ inline CyclicLanczosResult find_nullspace_cyclic_lanczos_ex(const MatrixInterfac
     throw std::invalid_argument(
         "find_nullspace_cyclic_lanczos: the B200 engine needs a CudaCsrMatrixAdapter and a CudaVectorFactory");
   if (opt.precond_AAt)
-    throw std::invalid_argument("find_nullspace_cyclic_lanczos: precond_AAt is not supported by the device engine");
+    throw std::invalid_argument("find_nullspace_cyclic_lanczos: host precond_AAt callbacks cannot run inside "
+                                "the device engine; use precond_device (KRANS_PRECOND_JACOBI or KRANS_PRECOND_SD)");
   krans_cyclic_opts o;
   krans_cyclic_opts_init(&o);
   o.k = (int64_t)opt.k;
@@ -98,6 +101,8 @@ inline CyclicLanczosResult find_nullspace_cyclic_lanczos_ex(const MatrixInterfac
   o.precision = opt.precision;
   o.team = opt.team;
   o.polish_block = opt.polish_block;
+  o.precond_aat = opt.precond_device;
+  o.precond_steps = opt.precond_steps;
   const krans_vec *y0 = nullptr;
   if (!opt.initial_right_space.empty() && opt.initial_right_space.front()) {
     const auto *c = dynamic_cast<const cuda::CudaVectorAdapter *>(opt.initial_right_space.front().get());

@@ -39,6 +39,8 @@ struct LOBPCGOptions {
   bool verbose = false;
   std::size_t progress_every = 100;
   int team = KRANS_TEAM_AUTO; // B200 engine knob
+  int precond_device = KRANS_PRECOND_NONE; // device form of M_inv (KRANS_PRECOND_JACOBI / _SD)
+  int precond_steps = 6;
 };
 
 struct LOBPCGResult {
@@ -62,7 +64,8 @@ inline LOBPCGResult find_nullspace_lobpcg_ex(const MatrixInterface &A, const Vec
     throw std::invalid_argument(
         "find_nullspace_lobpcg: the B200 engine needs a CudaCsrMatrixAdapter and a CudaVectorFactory");
   if (opt.M_inv)
-    throw std::invalid_argument("find_nullspace_lobpcg: M_inv is not supported by the device engine");
+    throw std::invalid_argument("find_nullspace_lobpcg: host M_inv callbacks cannot run inside the device "
+                                "engine; use precond_device (KRANS_PRECOND_JACOBI or KRANS_PRECOND_SD)");
   krans_lobpcg_opts o;
   krans_lobpcg_opts_init(&o);
   o.nev = (int64_t)opt.nev;
@@ -81,6 +84,8 @@ inline LOBPCGResult find_nullspace_lobpcg_ex(const MatrixInterface &A, const Vec
   o.verbose = opt.verbose;
   o.progress_every = (int64_t)opt.progress_every;
   o.team = opt.team;
+  o.precond_normal = opt.precond_device;
+  o.precond_steps = opt.precond_steps;
   std::vector<const krans_vec *> init;
   for (const auto &v : opt.initial_block) {
     const auto *c = dynamic_cast<const cuda::CudaVectorAdapter *>(v.get());

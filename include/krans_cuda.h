@@ -162,6 +162,23 @@ int krans_rng_seed(const krans_rng *r, uint32_t *seed);
 #define KRANS_TEAM_CTA 1  /* one thread block runs the solve */
 #define KRANS_TEAM_GRID 2 /* the whole GPU runs the solve (cooperative launch) */
 
+/* Device preconditioners for the CG projector on A A^T (precond_AAt,
+ * CyclicLanczosSolver.hpp:115) and for LOBPCG's N = A^T A (M_inv,
+ * LOBPCGSolver.hpp:98). The reference takes host callbacks, which a solver
+ * running whole on the GPU cannot call; these are the callbacks its own tests
+ * use, computed on the device:
+ *   KRANS_PRECOND_NONE     z = r (also the tests' identity callback)
+ *   KRANS_PRECOND_JACOBI   z_i = r_i / diag_i (diag of A A^T: squared row norms;
+ *                          of A^T A: squared column norms; 1 where the diagonal is 0)
+ *   KRANS_PRECOND_SD       precond_steps steps of steepest descent on the operator
+ *                          from z = 0 (tests/test_cyclic_lanczos.cpp:339-377,
+ *                          tests/test_lobpcg.cpp:179-205): q = r; per step
+ *                          alpha = q.q / q.Oq, z += alpha q, q -= alpha Oq, stopping
+ *                          when |q.Oq| < 1e-30 or q.q <= 1e-30 */
+#define KRANS_PRECOND_NONE 0
+#define KRANS_PRECOND_JACOBI 1
+#define KRANS_PRECOND_SD 2
+
 typedef struct krans_cyclic_opts {
   int64_t k;                 /* 1    number of right null vectors wanted */
   int64_t ncv;               /* 48   Krylov dimension (Lanczos vectors of H(A)) */
@@ -186,6 +203,8 @@ typedef struct krans_cyclic_opts {
   /* B200 engine knobs (no reference counterpart) */
   int32_t precision;         /* KRANS_PREC_FP64 */
   int32_t team;              /* KRANS_TEAM_AUTO */
+  int32_t precond_aat;       /* KRANS_PRECOND_NONE: the device form of precond_AAt */
+  int32_t precond_steps;     /* steps of KRANS_PRECOND_SD (8) */
   int32_t polish_block;      /* 0: polish candidates one by one (the reference's order);
                                 1: project up to 8 candidates of a restart with one block CG
                                 (matrix read once per iteration for all of them) */
@@ -224,6 +243,8 @@ typedef struct krans_lobpcg_opts {
   int64_t progress_every;    /* 100 (device engine: ignored) */
   int32_t precision;         /* KRANS_PREC_FP64 */
   int32_t team;              /* KRANS_TEAM_AUTO */
+  int32_t precond_normal;    /* KRANS_PRECOND_NONE: the device form of M_inv */
+  int32_t precond_steps;     /* steps of KRANS_PRECOND_SD (6) */
 } krans_lobpcg_opts;
 
 typedef struct krans_lobpcg_result {

@@ -22,6 +22,9 @@ KRANS_RNG_MT19937 = 0
 KRANS_RNG_PHILOX = 1
 KRANS_PREC_FP64 = 0
 KRANS_PREC_MIXED = 1
+KRANS_PRECOND_NONE = 0
+KRANS_PRECOND_JACOBI = 1
+KRANS_PRECOND_SD = 2
 KRANS_FMT_AUTO = 0
 KRANS_FMT_MTX = 1
 KRANS_FMT_IJA = 2
@@ -50,7 +53,7 @@ class CyclicOpts(C.Structure):
                 ("frob_samples", C.c_int32), ("prescreen_factor", C.c_double),
                 ("stagnation_restarts", C.c_int64), ("return_left_space", C.c_int32),
                 ("verbose", C.c_int32), ("precision", C.c_int32), ("team", C.c_int32),
-                ("polish_block", C.c_int32)]
+                ("precond_aat", C.c_int32), ("precond_steps", C.c_int32), ("polish_block", C.c_int32)]
 
 
 class CyclicResultC(C.Structure):
@@ -68,7 +71,8 @@ class LobpcgOpts(C.Structure):
                 ("restart", C.c_double), ("gs_tol", C.c_double), ("gs_reorth", C.c_int32),
                 ("frob_samples", C.c_int32), ("max_tiny_dim", C.c_int64),
                 ("nullity_known", C.c_int32), ("rank_known", C.c_int32), ("verbose", C.c_int32),
-                ("progress_every", C.c_int64), ("precision", C.c_int32), ("team", C.c_int32)]
+                ("progress_every", C.c_int64), ("precision", C.c_int32), ("team", C.c_int32),
+                ("precond_normal", C.c_int32), ("precond_steps", C.c_int32)]
 
 
 class LobpcgResultC(C.Structure):

@@ -319,6 +319,8 @@ class CyclicLanczosOptions:
     # engine knobs (no reference counterpart)
     precision: Precision = Precision.FP64
     team: int = K.KRANS_TEAM_AUTO
+    precond_aat: int = K.KRANS_PRECOND_NONE  # device form of precond_AAt (JACOBI or SD)
+    precond_steps: int = 8                   # steps of the SD preconditioner
     polish_block: int = 0  # 1: block CG polish of up to 8 candidates at once
 
     def to_c(self) -> K.CyclicOpts:
@@ -367,6 +369,8 @@ class LOBPCGOptions:
     progress_every: int = 100
     precision: Precision = Precision.FP64
     team: int = K.KRANS_TEAM_AUTO
+    precond_normal: int = K.KRANS_PRECOND_NONE  # device form of M_inv (JACOBI or SD)
+    precond_steps: int = 6                      # steps of the SD preconditioner
 
     def to_c(self) -> K.LobpcgOpts:
         o = K.LobpcgOpts()

@@ -110,6 +110,9 @@ struct BatchLaunch {
         trivial = 1;
       const int64_t ncv = std::max<int64_t>(std::max<int64_t>(2, r.opts.ncv), kt + 2);
       KR_CHECK_ARG(kt <= 128 && ncv <= 256, "krans_solve_batch: k <= 128 and ncv <= 256 per request");
+      KR_CHECK_ARG(r.opts.precond_aat >= KRANS_PRECOND_NONE && r.opts.precond_aat <= KRANS_PRECOND_SD &&
+                       r.opts.precond_steps >= 1 && r.opts.precond_steps <= 1000,
+                   "krans_solve_batch: precond_aat must be a KRANS_PRECOND_* value, precond_steps in [1, 1000]");
       if (!trivial)
         KR_CHECK_ARG(r.basis_out && r.basis_capacity >= kt, "krans_solve_batch: basis_out too small");
       q.trivial = trivial;
@@ -125,6 +128,7 @@ struct BatchLaunch {
       q.plan.grid_blocks = 1;
       q.plan.own_basis = 0;
       q.plan.block_polish = r.opts.polish_block ? 1 : 0;
+      q.plan.precond = r.opts.precond_aat;
       q.basis = r.basis_out;
       if (!trivial) {
         if (pos < n_large)

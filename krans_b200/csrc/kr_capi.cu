@@ -754,6 +754,8 @@ int krans_cyclic_opts_init(krans_cyclic_opts *o) {
   o->verbose = 0;
   o->precision = KRANS_PREC_FP64;
   o->team = KRANS_TEAM_AUTO;
+  o->precond_aat = KRANS_PRECOND_NONE;
+  o->precond_steps = 8;
   o->polish_block = 0;
   return KRANS_OK;
 }
@@ -777,6 +779,8 @@ int krans_lobpcg_opts_init(krans_lobpcg_opts *o) {
   o->progress_every = 100;
   o->precision = KRANS_PREC_FP64;
   o->team = KRANS_TEAM_AUTO;
+  o->precond_normal = KRANS_PRECOND_NONE;
+  o->precond_steps = 6;
   return KRANS_OK;
 }
 

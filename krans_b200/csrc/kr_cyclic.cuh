@@ -141,8 +141,13 @@ template <class Team, class KT> struct CyclicSolver {
   // are never needed (same value in exact arithmetic; rounding differs).
   // r and p are stored interleaved, so the gather of r + beta p at each entry
   // of F^T is one 16-byte load.
+  // `precond`: use the request's precond_aat (the candidate polish does; the
+  // random-projector fallback of try_project_random does not,
+  // CyclicLanczosSolver.cpp:140-214).
   __device__ __noinline__ int64_t cg(const double *rhs, double *u, int64_t maxit, double rel_tol, double bd_tol,
-                                     double *rnorm_out) {
+                                     double *rnorm_out, bool precond = true) {
+    if (precond && d.o.precond_aat != KRANS_PRECOND_NONE)
+      return cg_pre(rhs, u, maxit, rel_tol, bd_tol, rnorm_out);
     double2 *rp = d.rp;
     double *Ap = d.Ap, *tn = d.tn;
     double rr = 0.0;
@@ -238,6 +243,156 @@ template <class Team, class KT> struct CyclicSolver {
       });
       rzn = tm.sum1(rzn); // its barrier also publishes r for the next gather
       c.bytes += 24.0 * m + 24.0 * n;
+      if (!isfinite(rzn))
+        break;
+      rnorm = sqrt(rzn > 0.0 ? rzn : 0.0);
+      if (rnorm <= tol) {
+        ++k;
+        break;
+      }
+      beta = rzn / fmax(1e-300, rz);
+      rz = rzn;
+    }
+    *rnorm_out = rnorm;
+    return k;
+  }
+
+  // Jacobi weights 1 / diag(F F^T) (squared row norms of F; 1 for empty rows)
+  __device__ __noinline__ void jacobi_weights() {
+    team_for(tm, m, [&](int64_t i) {
+      double s2 = 0.0;
+      for (int32_t k = d.F.rp[i]; k < d.F.rp[i + 1]; k++) {
+        const double v = d.F.v64[k];
+        s2 += v * v;
+      }
+      d.dinv[i] = s2 > 0.0 ? 1.0 / s2 : 1.0;
+    });
+    c.bytes += 4.0 * m + 12.0 * d.F.nnz + 8.0 * m;
+    tm.sync();
+  }
+
+  // z = M^-1 r into zp[i].x: Jacobi (z = r / diag(F F^T)) or precond_steps
+  // steps of steepest descent on F F^T from z = 0 (the precond_AAt callback of
+  // tests/test_cyclic_lanczos.cpp:339-377: residual and direction coincide at
+  // the start of each step, so one vector q carries both)
+  __device__ __noinline__ void apply_precond(const double *r, double2 *zp) {
+    if (d.o.precond_aat == KRANS_PRECOND_JACOBI) {
+      team_for(tm, m, [&](int64_t i) { zp[i].x = d.dinv[i] * r[i]; });
+      c.bytes += 32.0 * m;
+      tm.sync();
+      return;
+    }
+    double *q = d.sd_q, *Oq = d.sd_Oq, *tn = d.tn;
+    team_for(tm, m, [&](int64_t i) {
+      zp[i].x = 0.0;
+      q[i] = r[i];
+    });
+    c.bytes += 24.0 * m;
+    tm.sync();
+    for (int it = 0; it < d.o.precond_steps && tm.ok(); it++) {
+      mulB(q, tn);
+      double acc[2] = {0.0, 0.0}; // q.Oq, q.q
+      csr_mv(tm, d.F, d.F.v64, tn, [&](int64_t i, double s) {
+        Oq[i] = s;
+        const double qi = q[i];
+        acc[0] += qi * s;
+        acc[1] += qi * qi;
+      });
+      count_F();
+      c.bytes += spmv_bytes(d.F.rows, d.F.cols, d.F.nnz, 8, 8, 8) + 8.0 * m;
+      tm.template sum<2>(acc);
+      if (!(fabs(acc[0]) >= 1e-30))
+        break;
+      const double alpha = acc[1] / acc[0];
+      double q2 = 0.0;
+      team_for(tm, m, [&](int64_t i) {
+        const double qi = q[i];
+        zp[i].x += alpha * qi;
+        const double qn = qi - alpha * Oq[i];
+        q[i] = qn;
+        q2 += qn * qn;
+      });
+      c.bytes += 48.0 * m;
+      q2 = tm.sum1(q2);
+      if (q2 <= 1e-30)
+        break;
+    }
+  }
+
+  // Preconditioned CG (cg_normal_eq_prec, CyclicLanczosSolver.cpp:48-113):
+  // z = M^-1 r, rz = r.z, p = z, tolerance on sqrt(r.z); otherwise as cg()
+  // (u = F^T w returned, direction update folded into the SpMVs, z and p
+  // interleaved for the gather of z + beta p).
+  __device__ __noinline__ int64_t cg_pre(const double *rhs, double *u, int64_t maxit, double rel_tol,
+                                         double bd_tol, double *rnorm_out) {
+    double2 *zp = d.rp;
+    double *r = d.r_pre, *Ap = d.Ap, *tn = d.tn;
+    double rr = 0.0;
+    team_for(tm, n, [&](int64_t i) { u[i] = 0.0; });
+    team_for(tm, m, [&](int64_t i) {
+      const double x = rhs[i];
+      r[i] = x;
+      rr += x * x;
+    });
+    rr = tm.sum1(rr);
+    c.bytes += 16.0 * m + 8.0 * n;
+    const double rhsn = sqrt(rr > 0.0 ? rr : 0.0);
+    *rnorm_out = rhsn;
+    if (!(rhsn > 0.0) || !isfinite(rhsn))
+      return 0;
+    apply_precond(r, zp);
+    double rz = 0.0;
+    team_for(tm, m, [&](int64_t i) {
+      const double z = zp[i].x;
+      zp[i].y = z;
+      rz += r[i] * z;
+    });
+    rz = tm.sum1(rz);
+    c.bytes += 32.0 * m;
+    if (!(rz > 0.0) || !isfinite(rz))
+      return 0;
+    double rnorm = sqrt(rz);
+    const double tol = fmax(rel_tol * rnorm, 1e-30);
+    *rnorm_out = rnorm;
+    if (rnorm <= tol)
+      return 0;
+    int64_t k = 0;
+    double beta = 0.0;
+    for (; k < maxit && tm.ok(); ++k) {
+      const double bq = beta;
+      team_spmv_x(
+          tm, d.B.rows, d.B.rp, d.B.ci, d.B.v64,
+          [&](int32_t cc) {
+            const double2 q = zp[cc];
+            return q.x + bq * q.y;
+          },
+          d.B.lanes, d.B.ulen, [&](int64_t i, double s) { tn[i] = s; });
+      count_B();
+      c.bytes += spmv_bytes(d.B.rows, d.B.cols, d.B.nnz, 8, 16, 8);
+      tm.sync();
+      double pap = 0.0;
+      csr_mv(tm, d.F, d.F.v64, tn, [&](int64_t i, double s) {
+        const double2 q = zp[i];
+        const double pn = q.x + bq * q.y;
+        zp[i].y = pn;
+        Ap[i] = s;
+        pap += pn * s;
+      });
+      count_F();
+      c.bytes += spmv_bytes(d.F.rows, d.F.cols, d.F.nnz, 8, 8, 8) + 24.0 * m;
+      pap = tm.sum1(pap);
+      if (!isfinite(pap) || fabs(pap) <= bd_tol)
+        break;
+      const double alpha = rz / pap;
+      team_for(tm, m, [&](int64_t i) { r[i] -= alpha * Ap[i]; });
+      team_for(tm, n, [&](int64_t i) { u[i] += alpha * tn[i]; });
+      c.bytes += 24.0 * m + 24.0 * n;
+      tm.sync();
+      apply_precond(r, zp);
+      double rzn = 0.0;
+      team_for(tm, m, [&](int64_t i) { rzn += r[i] * zp[i].x; });
+      rzn = tm.sum1(rzn); // its barrier also publishes z for the next gather
+      c.bytes += 16.0 * m;
       if (!isfinite(rzn))
         break;
       rnorm = sqrt(rzn > 0.0 ? rzn : 0.0);
@@ -415,7 +570,7 @@ template <class Team, class KT> struct CyclicSolver {
     const double tnorm = mulF_norm(v, tmv);
     double rn;
     double *u = d.vp;
-    const int64_t its = cg(tmv, u, 500, 1e-12, 1e-30, &rn);
+    const int64_t its = cg(tmv, u, 500, 1e-12, 1e-30, &rn, false);
     if (its > 0 || rn < tnorm) {
       team_for(tm, n, [&](int64_t i) { v[i] -= u[i]; });
       tm.sync();
@@ -782,6 +937,8 @@ template <class Team, class KT> struct CyclicSolver {
 
     const uint64_t t_run0 = globaltimer_ns();
     frob = fro_est();
+    if (d.o.precond_aat == KRANS_PRECOND_JACOBI)
+      jacobi_weights();
     const double fmx = fmax(1.0, frob);
     const double accept = fmax(o.tol_abs, o.tol_rel * fmx);
     const double prescreen = fmax(0.0, o.prescreen_factor) * fmx;
@@ -912,7 +1069,7 @@ template <class Team, class KT> struct CyclicSolver {
       bool have_best = false, accepted_this = false, polish_stalled = false;
       int64_t tested = 0;
       const int ny_used = split ? ncand : (l + 1) / 2;
-      if (d.Vc) {
+      if (d.Vc && d.o.precond_aat == KRANS_PRECOND_NONE) {
         CandState st{best_res, have_best, accepted_this, polish_stalled, converged};
         candidates_block(Y, split, l, ncand, test_cap, ny_used, prescreen, accept, st);
         best_res = st.best_res;
@@ -921,7 +1078,7 @@ template <class Team, class KT> struct CyclicSolver {
         converged = st.converged;
         tested = test_cap; // the one-by-one loop below is skipped
       }
-      for (int t = 0; t < ncand && tested < test_cap && tm.ok() && !d.Vc; ++t) {
+      for (int t = 0; t < ncand && tested < test_cap && tm.ok() && !(d.Vc && d.o.precond_aat == KRANS_PRECOND_NONE); ++t) {
         const int jb = *(volatile int32_t *)&d.ord[t];
         double ce2 = 0.0;
         for (int q = 0; q < ny_used; q++) {

@@ -114,6 +114,73 @@ template <class Team> struct LobpcgSolver {
     }
   }
 
+  // Jacobi weights of N = A^T A: 1 / squared column norms of A (rows of the
+  // stored transpose; 1 for empty columns)
+  __device__ __noinline__ void jacobi_weights_n() {
+    team_for(tm, n, [&](int64_t i) {
+      double s2 = 0.0;
+      for (int32_t k = d.B.rp[i]; k < d.B.rp[i + 1]; k++) {
+        const double v = d.B.v64[k];
+        s2 += v * v;
+      }
+      d.pc_dinv[i] = s2 > 0.0 ? 1.0 / s2 : 1.0;
+    });
+    c.bytes += 4.0 * n + 12.0 * d.B.nnz + 8.0 * n;
+    tm.sync();
+  }
+  // y = M^-1 x for N = A^T A (n-vectors, y != x): the device form of M_inv.
+  // Jacobi, or precond_steps steps of steepest descent on N from y = 0 (the
+  // M_inv callback of tests/test_lobpcg.cpp:179-205: the residual q is also
+  // the next direction). With no preconditioner y = x.
+  __device__ __noinline__ void apply_minv(const double *x, double *y) {
+    const int kind = d.o.precond_normal;
+    if (kind == KRANS_PRECOND_JACOBI) {
+      team_for(tm, n, [&](int64_t i) { y[i] = d.pc_dinv[i] * x[i]; });
+      c.bytes += 24.0 * n;
+      tm.sync();
+      return;
+    }
+    if (kind != KRANS_PRECOND_SD) {
+      copy(x, y);
+      return;
+    }
+    double *q = d.pc_q, *Nq = d.pc_nq;
+    team_for(tm, n, [&](int64_t i) {
+      y[i] = 0.0;
+      q[i] = x[i];
+    });
+    c.bytes += 24.0 * n;
+    tm.sync();
+    for (int it = 0; it < d.o.precond_steps && tm.ok(); it++) {
+      mulA(q, d.pc_tm);
+      double acc[2] = {0.0, 0.0}; // q.Nq, q.q
+      csr_mv(tm, d.B, d.B.v64, d.pc_tm, [&](int64_t i, double s) {
+        Nq[i] = s;
+        const double qi = q[i];
+        acc[0] += qi * s;
+        acc[1] += qi * qi;
+      });
+      c.spmvT++;
+      c.bytes += spmv_bytes(d.B.rows, d.B.cols, d.B.nnz, 8, 8, 8) + 8.0 * n;
+      tm.template sum<2>(acc);
+      if (!(fabs(acc[0]) >= 1e-30))
+        break;
+      const double alpha = acc[1] / acc[0];
+      double q2 = 0.0;
+      team_for(tm, n, [&](int64_t i) {
+        const double qi = q[i];
+        y[i] += alpha * qi;
+        const double qn = qi - alpha * Nq[i];
+        q[i] = qn;
+        q2 += qn * qn;
+      });
+      c.bytes += 48.0 * n;
+      q2 = tm.sum1(q2);
+      if (q2 <= 1e-30)
+        break;
+    }
+  }
+
   // MGS with optional reorth (GramSchmidt.cpp:55-82) on k columns of block V.
   __device__ __noinline__ bool mgs(double *V, int64_t k, double tol, bool reorth) {
     const uint64_t t0 = globaltimer_ns();
@@ -470,7 +537,7 @@ template <class Team> struct LobpcgSolver {
       if (res <= target)
         return true;
       mulAT(Av, t);
-      copy(t, dd);
+      apply_minv(t, dd); // d = M^-1 t (or t)
       gs_pass_excl(V, k, idx, dd);
       const double nd = nrm(dd);
       if (nd <= 1e-14)
@@ -543,6 +610,10 @@ template <class Team> struct LobpcgSolver {
         if (res <= target)
           continue;
         mulAT(r, g);
+        if (d.o.precond_normal != KRANS_PRECOND_NONE) {
+          apply_minv(g, d.vacc); // g <- M^-1 g
+          copy(d.vacc, g);
+        }
         gs_pass(d.Vb, k, g);
         const double gn = nrm(g);
         if (gn <= 1e-14)
@@ -649,6 +720,8 @@ template <class Team> struct LobpcgSolver {
       }
       R.frob = sqrt(sum2 / (double)samples);
     }
+    if (o.precond_normal == KRANS_PRECOND_JACOBI)
+      jacobi_weights_n();
     const double accept_thr = fmax(o.tol_abs, o.tol_rel * fmax(1.0, R.frob));
     R.accept = accept_thr;
 
@@ -765,9 +838,9 @@ template <class Team> struct LobpcgSolver {
         continue;
       }
 
-      // W = R (no preconditioner on the device engine)
+      // W = M^-1 R (LOBPCGSolver.cpp:655-656), W = R without M_inv
       for (int64_t j = ini; j < bs; j++)
-        copy(col(Rb, j), col(W, j));
+        apply_minv(col(Rb, j), col(W, j));
       const int64_t na = bs - ini;
       for (int64_t t = 0; t < na; t++)
         copy(col(W, ini + t), col(T1, t));

@@ -64,6 +64,9 @@ static int run_cyclic(krans_ctx *ctx, const krans_mat *A, bool trans, krans_rng 
   }
   KR_CHECK_ARG(k_target <= 128, "cyclic: at most 128 null vectors per request");
   KR_CHECK_ARG(ncv <= 256, "cyclic: ncv must be <= 256");
+  KR_CHECK_ARG(o.precond_aat >= KRANS_PRECOND_NONE && o.precond_aat <= KRANS_PRECOND_SD && o.precond_steps >= 1 &&
+                   o.precond_steps <= 1000,
+               "cyclic: precond_aat must be a KRANS_PRECOND_* value, precond_steps in [1, 1000]");
   int team = o.team;
   if (team == KRANS_TEAM_AUTO)
     team = (F.rows + F.cols) < 120000 ? KRANS_TEAM_CTA : KRANS_TEAM_GRID;
@@ -83,6 +86,7 @@ static int run_cyclic(krans_ctx *ctx, const krans_mat *A, bool trans, krans_rng 
   p.grid_blocks = grid ? cyclic_grid_blocks(ctx, mixed, threads) : 1;
   p.own_basis = grid ? 1 : 0;
   p.block_polish = o.polish_block ? 1 : 0;
+  p.precond = o.precond_aat;
   // one allocation: solver workspace, basis, request record and counters
   char *slot = nullptr;
   double *basis = nullptr, *d_mr = nullptr;
@@ -274,6 +278,8 @@ extern "C" int krans_solve_cyclic(krans_ctx *ctx, const krans_mat *A, krans_rng 
     lo.precision = o.precision;
     lo.team = o.team;
     lo.polish_block = o.polish_block;
+    lo.precond_aat = o.precond_aat;
+    lo.precond_steps = o.precond_steps;
     if (o.rank_known >= 0) {
       const int left_nullity = (int)A->m - o.rank_known;
       lo.nullity_known = std::max(0, std::min(left_nullity, (int)o.k));

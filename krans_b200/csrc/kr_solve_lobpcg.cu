@@ -72,6 +72,10 @@ static size_t lobpcg_layout(int64_t m, int64_t n, int64_t bs, int64_t k, int64_t
   t.sv_ad = c.take<double>(ldm);
   t.sv_nd = c.take<double>(ldn);
   t.sv_vn = c.take<double>(ldn);
+  t.pc_q = c.take<double>(ldn);
+  t.pc_nq = c.take<double>(ldn);
+  t.pc_dinv = c.take<double>(ldn);
+  t.pc_tm = c.take<double>(ldm);
   t.status = c.take<int32_t>(1);
   t.res = c.take<LobpcgDevResult>(1);
   t.gb = c.take<GridBarrierState>(1);
@@ -155,6 +159,9 @@ extern "C" int krans_solve_lobpcg(krans_ctx *ctx, const krans_mat *A, krans_rng 
   const int64_t guards =
       (bs == 1) ? 0 : std::min<int64_t>((int64_t)((1.0 - o.restart) * (double)bs + 0.45), bs - 1);
   KR_CHECK_ARG(bs <= 128, "krans_solve_lobpcg: block_size above 128 is not supported");
+  KR_CHECK_ARG(o.precond_normal >= KRANS_PRECOND_NONE && o.precond_normal <= KRANS_PRECOND_SD &&
+                   o.precond_steps >= 1 && o.precond_steps <= 1000,
+               "krans_solve_lobpcg: precond_normal must be a KRANS_PRECOND_* value, precond_steps in [1, 1000]");
   KR_CHECK_ARG(k_target <= 512, "krans_solve_lobpcg: more than 512 null vectors");
   if (n_initial > 0)
     KR_CHECK_ARG(initial_block != nullptr, "krans_solve_lobpcg: initial_block is NULL");

@@ -68,6 +68,7 @@ struct CyclicDesc {
   double *Hb, *Wb, *Rk, *Pk, *Ak, *Tk; // interleaved CG blocks: m x KR_NBP (Tk: n x KR_NBP)
   double *tmv, *wm, *Ap;             // m-vectors
   double2 *rp;                       // CG residual and direction, interleaved (m)
+  double *r_pre, *dinv, *sd_q, *sd_Oq; // preconditioned CG: residual, Jacobi weights, SD vectors (m)
   double *alpha, *beta;              // ncv + 2
   double *Tb, *Vt, *sv;              // tiny problem
   int32_t *ord;
@@ -89,6 +90,7 @@ struct CyclicPlan {
   int32_t grid_blocks; // blocks of a grid team (reduction partials)
   int32_t own_basis;   // basis lives in the workspace (else in the request)
   int32_t block_polish; // workspace for the block CG polish (KR_NBP candidates at once)
+  int32_t precond;      // KRANS_PRECOND_* of the CG projector (workspace for it)
 };
 
 __host__ __device__ inline int64_t kr_round_up(int64_t x, int64_t a) { return (x + a - 1) / a * a; }
@@ -133,6 +135,13 @@ __host__ __device__ inline size_t cyclic_carve(const CyclicPlan &p, char *base, 
   CyclicDevResult *res = c.take<CyclicDevResult>(1);
   GridBarrierState *gb = c.take<GridBarrierState>(1);
   double *gpart = c.take<double>(2 * (p.grid_blocks > 1 ? p.grid_blocks : 1) * KR_RED_K);
+  double *r_pre = nullptr, *dinv = nullptr, *sd_q = nullptr, *sd_Oq = nullptr;
+  if (p.precond) {
+    r_pre = c.take<double>(p.ldm);
+    dinv = c.take<double>(p.ldm);
+    sd_q = c.take<double>(p.ldm);
+    sd_Oq = c.take<double>(p.ldm);
+  }
   double *Vc = nullptr, *Hb = nullptr, *Wb = nullptr, *Rk = nullptr, *Pk = nullptr, *Ak = nullptr, *Tk = nullptr;
   if (p.block_polish) {
     Vc = c.take<double>(KR_NBP * p.ldn);
@@ -153,6 +162,7 @@ __host__ __device__ inline size_t cyclic_carve(const CyclicPlan &p, char *base, 
     if (p.own_basis) { d->status = status; d->res = res; }
     d->gb = gb; d->gpart = gpart;
     d->Vc = Vc; d->Hb = Hb; d->Wb = Wb; d->Rk = Rk; d->Pk = Pk; d->Ak = Ak; d->Tk = Tk;
+    d->r_pre = r_pre; d->dinv = dinv; d->sd_q = sd_q; d->sd_Oq = sd_Oq;
     d->ldn = p.ldn; d->ldm = p.ldm; d->ldb = p.ldb; d->cap = p.cap;
   }
   return c.off + 256;
@@ -214,6 +224,7 @@ struct LobpcgDesc {
   double *pr, *pg, *ptmp;              // m, n, m
   double *Vb, *D, *Vn, *Zp, *AZp;      // k, k+2, k, 2k+2, 2k+2 columns
   double *sv_av, *sv_t, *sv_d, *sv_ad, *sv_nd, *sv_vn; // sharpen scratch
+  double *pc_q, *pc_nq, *pc_dinv, *pc_tm;              // M_inv scratch (n, n, n, m)
   int64_t ldn, ldm, pmax;
   int32_t *status;
   LobpcgDevResult *res;
