@@ -555,8 +555,9 @@ def run_planted(args):
     A = inst.A
     L = lower_norm_bound(A)
     M = kb.CudaCsrMatrixAdapter.from_scipy(ctx, A, fp32=True)
-    opt = kb.CyclicLanczosOptions(k=k, tol_abs=1e-12 * L, tol_rel=0.0, cg_maxit=1000, ncv=args.ncv,
-                                  max_restarts=args.max_restarts, precision=kb.Precision.MIXED)
+    opt = kb.CyclicLanczosOptions(k=k, tol_abs=1e-12 * L, tol_rel=0.0, cg_maxit=args.cg_maxit, ncv=args.ncv,
+                                  max_restarts=args.max_restarts, stagnation_restarts=args.stagnation,
+                                  precision=kb.Precision.MIXED)
 
     def solve():
         R = kb.find_nullspace_cyclic_lanczos_ex(M, kb.CudaVectorFactory(ctx, A.shape[1], seed=42, mode="philox"),
@@ -572,10 +573,10 @@ def run_planted(args):
         "scaling": "strong", "vs_baseline": None, "dtype": "f32 SpMV/Krylov + f64 reorth/tiny-SVD/CG polish",
         "data": "synthetic",
         "config": {"workload": f"planted kernel A=[B|BW], m={m}, n={A.shape[1]}, k={k}", "nnz": A.nnz,
-                   "ncv": args.ncv, "max_restarts": args.max_restarts,
-                   "accept": "tol_abs=1e-12*max(row,col norm), tol_rel=0, cg_maxit=1000"},
+                   "ncv": args.ncv, "max_restarts": args.max_restarts, "stagnation_restarts": args.stagnation,
+                   "accept": f"tol_abs=1e-12*max(row,col norm), tol_rel=0, cg_maxit={args.cg_maxit}"},
         "found": U.shape[0], "converged": R.converged_to_target, "restarts": R.restarts,
-        "cg_solves": R.cg_solves, "max_rel_residual": worst,
+        "cg_solves": R.cg_solves, "cg_maxit_hits": R.cg_maxit_hits, "max_rel_residual": worst,
         "roofline": {"bound": "hbm", "achieved": R.algo_bytes / T / 1e9, "peak": peak,
                      "unit": "GB/s", "frac": R.algo_bytes / T / 1e9 / peak, "traffic": None},
         "phase_ms": list(R.phase_ms), "clocks": clocks, "gpu_launches": 1,
@@ -717,6 +718,8 @@ def main():
     ap.add_argument("--cpu-iters", type=int, default=3)
     ap.add_argument("--ncv", type=int, default=96)
     ap.add_argument("--max-restarts", type=int, default=400)
+    ap.add_argument("--cg-maxit", type=int, default=1000, help="planted: CG iteration cap of the projector")
+    ap.add_argument("--stagnation", type=int, default=30, help="planted: restarts without progress before stopping")
     ap.add_argument("--pool", type=int, default=64)
     ap.add_argument("--nnz-lo", type=float, default=1e4)
     ap.add_argument("--nnz-hi", type=float, default=2e6)
