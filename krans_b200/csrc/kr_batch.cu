@@ -39,7 +39,10 @@ struct BatchLaunch {
   int count = 0;
   int precision = 0;
   int grid = 0;        // CTA-team blocks (small requests)
-  int n_large = 0;     // requests [0, n_large) run on clusters
+  int n_large = 0;     // requests [0, n_large) run on clusters of csize blocks
+  int n_mid = 0;       // requests [n_large, n_large + n_mid) run on 2-block clusters (pairs)
+  int npairs = 0;      // pair clusters of the second launch (the SMs the big clusters leave free)
+  size_t stride_M = 0; // workspace slot of one pair
   size_t dyn_smem = 0; // dynamic shared memory per block (CG vectors of one-block solves)
   int csize = 8;       // blocks per cluster
   int nclusters = 0;   // resident clusters of the cluster launch
@@ -79,16 +82,38 @@ struct BatchLaunch {
       return (v >= 2 && v <= 16) ? v : 8;
     }();
     csize = cl_size;
-    auto is_large = [&](int a) { return reqs[a].A->m + reqs[a].A->n >= cluster_min && cluster_min > 0; };
+    // Size classes (by m + n only, so a request runs on the same kind of
+    // team, with the same rounding, in any batch): big ones on clusters of
+    // csize blocks; mid-size ones on 2-block clusters launched next to them
+    // on the SMs the big clusters cannot tile (a GPC holds whole clusters
+    // only); small ones on single blocks.
+    static const int64_t pair_max = [] {
+      const char *e = getenv("KRANS_PAIR_MAX");
+      return e ? atoll(e) : (int64_t)120000;
+    }();
+    const bool mixed_p = precision == KRANS_PREC_MIXED;
+    {
+      const int maxc = cyclic_batch_cluster_max(mixed_p, csize, ctx->sms, 0);
+      npairs = csize > 2 && pair_max > cluster_min ? std::max(0, (ctx->sms - maxc * csize) / 2) : 0;
+    }
+    auto cls = [&](int a) {
+      const int64_t sz = reqs[a].A->m + reqs[a].A->n;
+      if (cluster_min <= 0 || sz < cluster_min)
+        return 2;
+      return (npairs > 0 && sz < pair_max) ? 1 : 0;
+    };
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
-      const bool la = is_large(a), lb = is_large(b);
-      if (la != lb)
-        return la;
+      const int ca = cls(a), cb = cls(b);
+      if (ca != cb)
+        return ca < cb;
       return reqs[a].A->nnz > reqs[b].A->nnz;
     });
-    n_large = 0;
-    for (int pos = 0; pos < n; pos++)
-      n_large += is_large(order[pos]) ? 1 : 0;
+    n_large = n_mid = 0;
+    for (int pos = 0; pos < n; pos++) {
+      const int c = cls(order[pos]);
+      n_large += c == 0;
+      n_mid += c == 1;
+    }
     hreq.assign(n, CyclicRequestDev{});
     hrng.assign(n, RngState{});
     ws_stride = 256;
@@ -133,6 +158,8 @@ struct BatchLaunch {
       if (!trivial) {
         if (pos < n_large)
           stride_L = std::max(stride_L, cyclic_carve(q.plan, nullptr, nullptr));
+        else if (pos < n_large + n_mid)
+          stride_M = std::max(stride_M, cyclic_carve(q.plan, nullptr, nullptr));
         else
           ws_stride = std::max(ws_stride, cyclic_carve(q.plan, nullptr, nullptr));
       }
@@ -144,12 +171,13 @@ struct BatchLaunch {
     }
     ws_stride = (size_t)kr_round_up((int64_t)ws_stride, 256);
     stride_L = (size_t)kr_round_up((int64_t)std::max<size_t>(stride_L, 256), 256);
-    const int n_small = n - n_large;
+    stride_M = (size_t)kr_round_up((int64_t)std::max<size_t>(stride_M, 256), 256);
+    const int n_small = n - n_large - n_mid;
     const bool mixed = precision == KRANS_PREC_MIXED;
     // dynamic shared memory for the CG vectors of one-block solves: the
     // largest small request that fits under the cap
     dyn_smem = 0;
-    for (int pos = n_large; pos < n; pos++) {
+    for (int pos = n_large + n_mid; pos < n; pos++) {
       const size_t b = cta_cg_smem_bytes(hreq[pos].plan.ldm, hreq[pos].plan.ldn);
       if (b <= cta_smem_cap())
         dyn_smem = std::max(dyn_smem, b);
@@ -157,7 +185,9 @@ struct BatchLaunch {
     const int per_sm = cyclic_batch_cta_per_sm(mixed);
     grid = n_small > 0 ? std::max(1, std::min(n_small, ctx->sms * per_sm)) : 0;
     nclusters = 0;
-    if (n_large > 0) {
+    if (n_mid == 0)
+      npairs = 0;
+    if (n_large > 0 || n_mid > 0) {
       // one cluster launch fills the GPU; its blocks take the small requests
       // after the large queue is empty (one small-request slot per block)
       const int maxc = cyclic_batch_cluster_max(mixed, csize, ctx->sms, dyn_smem);
@@ -166,7 +196,8 @@ struct BatchLaunch {
     }
     meta_bytes = (size_t)n * (sizeof(CyclicRequestDev) + sizeof(CyclicDevResult) + 4 + 8 + sizeof(RngState)) +
                  4096;
-    ws_bytes = (size_t)grid * ws_stride + (size_t)nclusters * stride_L + 256;
+    ws_bytes = (size_t)(grid + 2 * npairs) * ws_stride + (size_t)nclusters * stride_L +
+               (size_t)npairs * stride_M + 256;
     *need = ws_bytes + meta_bytes;
     return KRANS_OK;
   }
@@ -190,7 +221,7 @@ struct BatchLaunch {
     d_status = c.take<int32_t>(count);
     d_mr = c.take<double>(count);
     d_rng = c.take<RngState>(count);
-    d_queue = c.take<int>(2);
+    d_queue = c.take<int>(4);
     for (int pos = 0; pos < count; pos++) {
       hreq[pos].res = d_res + pos;
       hreq[pos].status = d_status + pos;
@@ -217,17 +248,38 @@ struct BatchLaunch {
     if (e == cudaSuccess)
       e = cudaMemsetAsync(d_mr, 0, 8 * (size_t)count, s);
     if (e == cudaSuccess)
-      e = cudaMemsetAsync(d_queue, 0, 2 * sizeof(int), s);
+      e = cudaMemsetAsync(d_queue, 0, 4 * sizeof(int), s);
     if (e == cudaSuccess)
       e = cudaEventRecord(ev0, s);
-    char *ws_small = ws, *ws_large = ws + (size_t)grid * ws_stride;
+    char *ws_small = ws, *ws_small_p = ws + (size_t)grid * ws_stride;
+    char *ws_large = ws_small_p + (size_t)2 * npairs * ws_stride;
+    char *ws_mid = ws_large + (size_t)nclusters * stride_L;
     const bool mixed = precision == KRANS_PREC_MIXED;
+    const int first_small = n_large + n_mid;
+    if (e == cudaSuccess && npairs > 0) {
+      // the pair launch runs beside the big clusters on its own stream; the
+      // launch's end event waits for both
+      e = cudaStreamCreateWithFlags(&aux, cudaStreamNonBlocking);
+      if (e == cudaSuccess)
+        e = cudaEventCreateWithFlags(&evj, cudaEventDisableTiming);
+    }
+    if (e == cudaSuccess && npairs > 0)
+      e = cudaStreamWaitEvent(aux, ev0, 0); // the pairs start after the set-up copies
     if (e == cudaSuccess) {
-      if (n_large > 0)
+      if (n_large > 0 || n_mid > 0) {
         e = launch_cyclic_batch_cluster(mixed, nclusters, csize, dyn_smem, s, d_reqs, n_large, d_queue, ws_large,
-                                        stride_L,
-                                        d_reqs + n_large, count - n_large, d_queue + 1, ws_small, ws_stride);
-      else
+                                        stride_L, d_reqs + first_small, count - first_small, d_queue + 1,
+                                        ws_small, ws_stride);
+        if (e == cudaSuccess && npairs > 0) {
+          e = launch_cyclic_batch_cluster(mixed, npairs, 2, dyn_smem, aux, d_reqs + n_large, n_mid,
+                                            d_queue + 2, ws_mid, stride_M, d_reqs + first_small,
+                                            count - first_small, d_queue + 1, ws_small_p, ws_stride);
+          if (e == cudaSuccess)
+            e = cudaEventRecord(evj, aux);
+          if (e == cudaSuccess)
+            e = cudaStreamWaitEvent(s, evj, 0);
+        }
+      } else
         e = launch_cyclic_batch_cta(mixed, grid, 512, dyn_smem, s, d_reqs, count, d_queue + 1, ws_small, ws_stride);
     }
     if (e == cudaSuccess)
