@@ -146,6 +146,124 @@ KR_DEV void team_gemm_tn(Team &tm, int64_t n, const double *A, int a, const doub
   tm.sync();
 }
 
+// C = A^T B (a x b, leading dim a) for tall-skinny column-major A (n x a) and
+// B (n x b), leading dim ld, on the FP64 tensor cores with shared-memory
+// panels. Work items are (64 x 64 tile of C, fixed chunk of rows); a block
+// stages 16-row panels of the tile's 64 columns of A and of B in shared
+// memory, and each of its 16 warps accumulates a 16 x 16 piece (four DMMA
+// 8x8 tiles). Each item leaves its partial tile in `part`; the partials are
+// then summed in chunk order, so the result depends only on the team size
+// (which fixes the chunking), not on which block ran which item. `part` must
+// hold ceil(a/64) * ceil(b/64) * 4096 * nchunks doubles, nchunks <= ncta.
+// Blocks of 512 threads.
+#define KR_GT 64 // tile edge
+#define KR_GK 16 // rows per shared-memory panel
+template <class Team>
+KR_DEV void team_gemm_tn_tiled(Team &tm, int64_t n, const double *A, int a, const double *B, int b, int64_t ld,
+                               double *C, double *part) {
+  __shared__ double sA[KR_GT][KR_GK + 1], sB[KR_GT][KR_GK + 1];
+  const int ta = (a + KR_GT - 1) / KR_GT, tb = (b + KR_GT - 1) / KR_GT, nt = ta * tb;
+  const int ncta = tm.ncta();
+  const int64_t kblocks = (n + KR_GK - 1) / KR_GK;
+  const int nch = (int)imin64(imin64(ncta, kblocks > 0 ? kblocks : 1), (int64_t)(2 * ncta + nt - 1) / nt);
+  const int nchunks = nch > 0 ? nch : 1;
+  const int64_t kb_per = (kblocks + nchunks - 1) / nchunks; // panels per chunk
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int wr = (wid >> 2) * 16, wc = (wid & 3) * 16; // this warp's 16 x 16 piece
+  const int items = nt * nchunks;
+  for (int it = tm.cta_rank(); it < items; it += ncta) {
+    const int tile = it % nt, ch = it / nt;
+    const int ti = tile % ta, tj = tile / ta;
+    const int64_t kb0 = (int64_t)ch * kb_per, kb1 = imin64(kb0 + kb_per, kblocks);
+    double acc[2][2][2];
+#pragma unroll
+    for (int x = 0; x < 2; x++)
+#pragma unroll
+      for (int y = 0; y < 2; y++)
+        acc[x][y][0] = acc[x][y][1] = 0.0;
+    // panels travel global -> registers two ahead of use -> shared memory, so
+    // their loads are in flight while the tensor cores work on the current one
+    constexpr int PER = (2 * KR_GT * KR_GK + 511) / 512; // elements per thread and panel (512 threads)
+    auto fetch = [&](int64_t kb, double (&v)[PER]) {
+      const int64_t r0 = kb * KR_GK;
+#pragma unroll
+      for (int q = 0; q < PER; q++) {
+        const int e = threadIdx.x + q * 512;
+        const int which = e / (KR_GT * KR_GK), rem = e % (KR_GT * KR_GK);
+        const int c = rem / KR_GK, k = rem % KR_GK;
+        const int64_t r = r0 + k;
+        double x = 0.0;
+        if (e < 2 * KR_GT * KR_GK && kb < kb1 && r < n) {
+          const int col = (which == 0 ? ti : tj) * KR_GT + c;
+          if (col < (which == 0 ? a : b))
+            x = (which == 0 ? A : B)[(int64_t)col * ld + r];
+        }
+        v[q] = x;
+      }
+    };
+    double v0[PER], v1[PER];
+    fetch(kb0, v0);
+    fetch(kb0 + 1, v1);
+    for (int64_t kb = kb0; kb < kb1; kb++) {
+#pragma unroll
+      for (int q = 0; q < PER; q++) {
+        const int e = threadIdx.x + q * 512;
+        if (e < 2 * KR_GT * KR_GK) {
+          const int which = e / (KR_GT * KR_GK), rem = e % (KR_GT * KR_GK);
+          const int c = rem / KR_GK, k = rem % KR_GK;
+          if (which == 0)
+            sA[c][k] = v0[q];
+          else
+            sB[c][k] = v0[q];
+        }
+        v0[q] = v1[q];
+      }
+      __syncthreads();
+      fetch(kb + 2, v1);
+      if (wid < 16) {
+#pragma unroll
+        for (int kk = 0; kk < KR_GK; kk += 4) {
+          double fa[2], fb[2];
+#pragma unroll
+          for (int x = 0; x < 2; x++)
+            fa[x] = sA[wr + 8 * x + (lane >> 2)][kk + (lane & 3)];
+#pragma unroll
+          for (int y = 0; y < 2; y++)
+            fb[y] = sB[wc + 8 * y + (lane >> 2)][kk + (lane & 3)];
+#pragma unroll
+          for (int x = 0; x < 2; x++)
+#pragma unroll
+            for (int y = 0; y < 2; y++)
+              dmma_8x8x4(acc[x][y][0], acc[x][y][1], fa[x], fb[y]);
+        }
+      }
+      __syncthreads();
+    }
+    if (wid < 16) {
+      double *pt = part + (size_t)it * (KR_GT * KR_GT);
+#pragma unroll
+      for (int x = 0; x < 2; x++)
+#pragma unroll
+        for (int y = 0; y < 2; y++) {
+          const int i = wr + 8 * x + (lane >> 2), j = wc + 8 * y + 2 * (lane & 3);
+          pt[i + j * KR_GT] = acc[x][y][0];
+          pt[i + (j + 1) * KR_GT] = acc[x][y][1];
+        }
+    }
+  }
+  tm.sync();
+  const int64_t nthr = tm.nthreads();
+  for (int64_t e = tm.tid(); e < (int64_t)a * b; e += nthr) {
+    const int i = (int)(e % a), j = (int)(e / a);
+    const int tile = (i / KR_GT) + ta * (j / KR_GT), li = i % KR_GT, lj = j % KR_GT;
+    double s = 0.0;
+    for (int ch = 0; ch < nchunks; ch++)
+      s += __ldcg(part + (size_t)(tile + ch * nt) * (KR_GT * KR_GT) + li + lj * KR_GT);
+    C[e] = s;
+  }
+  tm.sync();
+}
+
 // X[:, i] -= sum_j S[:, j] * Cc(j, i) for i < k, j < ns (X, S column-major
 // with leading dim ld; Cc leading dim ldc).
 template <class Team>
