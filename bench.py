@@ -356,7 +356,8 @@ def run_ours(args):
     traffic = DRAM_PER_ALGO_BYTE * algo_bytes / max(1, len(dev_ms))
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                "kernel": "cyclic_batch_kernel + cyclic_batch_cluster_kernel (one launch per step)",
+                "kernel": "cyclic_batch_cluster_kernel (per step: one launch of 8-block clusters + one of 2-block "
+                          "clusters beside it; both take the single-block requests last)",
                 "algo_bytes_per_launch": algo_bytes / max(1, len(dev_ms))}
 
     line = {
