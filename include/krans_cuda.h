@@ -65,8 +65,12 @@ int krans_ctx_sm_count(const krans_ctx *ctx, int *sms);
 /* ---- CSR matrix: MatrixInterface (rows, cols, multiply, multiply_transpose) --
  * Replaces EigenSparseMatrixAdapter(A), which owns A and a cached transpose
  * (include/krans/adapters/eigen/EigenSparseMatrixAdapter.hpp:20-24,56).
- * Host arrays are copied; the transpose is built on the device. Column
- * indices within a row need not be sorted; duplicates are kept as given. */
+ * Host arrays are copied before the call returns (they may be reused at
+ * once); the transpose is then built on the device, asynchronously on the
+ * context's stream, which every entry point of this library orders against
+ * (work a caller queues on other streams with the raw device arrays must
+ * wait for that stream). Column indices within a row need not be sorted;
+ * duplicates are kept as given. */
 #define KRANS_CSR_FP64 1 /* keep FP64 values (needed by every FP64 path) */
 #define KRANS_CSR_FP32 2 /* also keep an FP32 copy of the values (mixed precision) */
 int krans_csr_create(krans_ctx *ctx, int64_t m, int64_t n, int64_t nnz,

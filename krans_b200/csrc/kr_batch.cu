@@ -437,6 +437,7 @@ struct krans_server {
   std::deque<uint64_t> queue;
   std::vector<cudaStream_t> streams;
   std::vector<bool> stream_busy;
+  cudaEvent_t ctx_ready = nullptr; // orders launches after work queued on the context's stream
   std::vector<InFlight *> inflight;
   size_t bytes_in_use = 0;
   uint64_t next_ticket = 1;
@@ -539,6 +540,15 @@ void krans_server::run() {
             queue.push_front(*it);
           delete f;
         } else {
+          // matrices finish their device set-up (transpose) on the context's
+          // stream: the launch's stream waits for it
+          if (rc == KRANS_OK) {
+            cudaError_t ew = cudaEventRecord(ctx_ready, ctx->stream);
+            if (ew == cudaSuccess)
+              ew = cudaStreamWaitEvent(streams[free_s], ctx_ready, 0);
+            if (ew != cudaSuccess)
+              rc = cuda_fail(ew, "server stream order", __FILE__, __LINE__);
+          }
           if (rc == KRANS_OK)
             rc = f->L.alloc_and_launch(streams[free_s]);
           const auto now = Clock::now();
@@ -612,9 +622,13 @@ int krans_server_create(krans_ctx *ctx, const krans_server_opts *opts, krans_ser
       s->stream_busy.push_back(false);
     }
   }
+  if (e == cudaSuccess)
+    e = cudaEventCreateWithFlags(&s->ctx_ready, cudaEventDisableTiming);
   if (e != cudaSuccess) {
     for (auto st : s->streams)
       cudaStreamDestroy(st);
+    if (s->ctx_ready)
+      cudaEventDestroy(s->ctx_ready);
     delete s;
     return cuda_fail(e, "server streams", __FILE__, __LINE__);
   }
@@ -641,6 +655,8 @@ int krans_server_destroy(krans_server *s) {
   }
   for (auto st : s->streams)
     cudaStreamDestroy(st);
+  if (s->ctx_ready)
+    cudaEventDestroy(s->ctx_ready);
   delete s;
   return KRANS_OK;
 }

@@ -350,58 +350,83 @@ int krans_csr_create(krans_ctx *ctx, int64_t m, int64_t n, int64_t nnz, const in
                "krans_csr_create: sizes must fit 32-bit indices");
   KR_CHECK_ARG(row_ptr && (nnz == 0 || (col_idx && values)), "krans_csr_create: NULL array");
   KR_CHECK_ARG(row_ptr[0] == 0 && row_ptr[m] == nnz, "krans_csr_create: row_ptr[0] != 0 or row_ptr[m] != nnz");
-  for (int64_t i = 0; i < m; i++)
-    KR_CHECK_ARG(row_ptr[i] <= row_ptr[i + 1], "krans_csr_create: row_ptr not monotone");
-  for (int64_t k = 0; k < nnz; k++)
-    KR_CHECK_ARG(col_idx[k] >= 0 && col_idx[k] < n, "krans_csr_create: column index out of range");
+  // one pass over the rows (monotone, uniform length) and one over the
+  // columns (range, per-column counts for the transpose's uniform length)
+  const int64_t L = m > 0 ? (int64_t)(row_ptr[1] - row_ptr[0]) : 0;
+  bool uni = m > 0 && L > 0 && L <= 8;
+  for (int64_t i = 0; i < m; i++) {
+    const int32_t len = row_ptr[i + 1] - row_ptr[i];
+    KR_CHECK_ARG(len >= 0, "krans_csr_create: row_ptr not monotone");
+    uni = uni && len == L;
+  }
+  std::vector<int32_t> cc((size_t)n, 0);
+  for (int64_t k = 0; k < nnz; k++) {
+    const int32_t c = col_idx[k];
+    KR_CHECK_ARG(c >= 0 && c < n, "krans_csr_create: column index out of range");
+    cc[(size_t)c]++;
+  }
+  const int32_t LT = n > 0 ? cc[0] : 0;
+  bool uniT = n > 0 && LT > 0 && LT <= 8;
+  for (int64_t j = 0; uniT && j < n; j++)
+    uniT = cc[(size_t)j] == LT;
   if (!(flags & (KRANS_CSR_FP64 | KRANS_CSR_FP32)))
     flags |= KRANS_CSR_FP64;
   flags |= KRANS_CSR_FP64; // FP64 values are kept for every path (polish, residuals)
   KR_CUDA(cudaSetDevice(ctx->device));
+  const bool f32 = (flags & KRANS_CSR_FP32) != 0;
+  const size_t sz_rp = (size_t)(m + 1) * 4, sz_rpT = (size_t)(n + 1) * 4, sz_ci = (size_t)std::max<int64_t>(nnz, 1) * 4;
+  const size_t sz_v = (size_t)std::max<int64_t>(nnz, 1) * 8, sz_v32 = (size_t)std::max<int64_t>(nnz, 1) * 4;
+  // the stored arrays share one allocation (carved at 256-byte offsets)
+  auto up = [](size_t x) { return (x + 255) & ~(size_t)255; };
+  const size_t total = up(sz_rp) + 2 * up(sz_ci) + 2 * up(sz_v) + up(sz_rpT) + (f32 ? 2 * up(sz_v32) : 0);
+  char *base = nullptr;
+  int rc = dev_alloc(ctx, (void **)&base, total);
+  if (rc != KRANS_OK)
+    return rc;
   auto *A = new krans_mat();
   A->ctx = ctx;
   A->m = m;
   A->n = n;
   A->nnz = nnz;
-  const size_t sz_rp = (size_t)(m + 1) * 4, sz_rpT = (size_t)(n + 1) * 4, sz_ci = (size_t)std::max<int64_t>(nnz, 1) * 4;
-  const size_t sz_v = (size_t)std::max<int64_t>(nnz, 1) * 8, sz_v32 = (size_t)std::max<int64_t>(nnz, 1) * 4;
-  int rc = KRANS_OK;
-  auto alloc = [&](void **p, size_t b) {
-    if (rc == KRANS_OK) {
-      rc = dev_alloc(ctx, p, b);
-      if (rc == KRANS_OK)
-        A->bytes += b;
-    }
+  A->base = base;
+  A->bytes = total;
+  size_t off = 0;
+  auto take = [&](size_t b) {
+    char *p = base + off;
+    off += up(b);
+    return p;
   };
-  alloc((void **)&A->rp, sz_rp);
-  alloc((void **)&A->ci, sz_ci);
-  alloc((void **)&A->v, sz_v);
-  alloc((void **)&A->rpT, sz_rpT);
-  alloc((void **)&A->ciT, sz_ci);
-  alloc((void **)&A->vT, sz_v);
-  if (flags & KRANS_CSR_FP32) {
-    alloc((void **)&A->v32, sz_v32);
-    alloc((void **)&A->vT32, sz_v32);
+  A->rp = (int32_t *)take(sz_rp);
+  A->ci = (int32_t *)take(sz_ci);
+  A->v = (double *)take(sz_v);
+  A->rpT = (int32_t *)take(sz_rpT);
+  A->ciT = (int32_t *)take(sz_ci);
+  A->vT = (double *)take(sz_v);
+  if (f32) {
+    A->v32 = (float *)take(sz_v32);
+    A->vT32 = (float *)take(sz_v32);
   }
-  int32_t *cnt = nullptr, *perm = nullptr, *tmp = nullptr, *rowof = nullptr;
-  alloc((void **)&cnt, sz_rpT);
-  alloc((void **)&perm, sz_ci);
-  alloc((void **)&tmp, sz_ci);
-  alloc((void **)&rowof, sz_ci);
-  if (rc != KRANS_OK) {
-    dev_free(ctx, cnt, sz_rpT);
-    dev_free(ctx, perm, sz_ci);
-    dev_free(ctx, tmp, sz_ci);
-    dev_free(ctx, rowof, sz_ci);
-    krans_csr_destroy(A);
-    return rc;
-  }
+  // scratch of the device transpose: stream-ordered, so releasing it does not
+  // wait for the device, and the next matrix's host work overlaps this
+  // matrix's transpose kernels
   cudaStream_t s = ctx->stream;
-  cudaError_t e = cudaMemcpyAsync(A->rp, row_ptr, sz_rp, cudaMemcpyHostToDevice, s);
+  int32_t *scratch = nullptr;
+  const size_t sz_scr = up(sz_rpT) + 3 * up(sz_ci);
+  cudaError_t e = cudaMallocAsync((void **)&scratch, sz_scr, s);
+  int32_t *cnt = scratch, *perm = (int32_t *)((char *)scratch + up(sz_rpT));
+  int32_t *tmp = (int32_t *)((char *)perm + up(sz_ci)), *rowof = (int32_t *)((char *)tmp + up(sz_ci));
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(A->rp, row_ptr, sz_rp, cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess && nnz)
     e = cudaMemcpyAsync(A->ci, col_idx, (size_t)nnz * 4, cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess && nnz)
     e = cudaMemcpyAsync(A->v, values, (size_t)nnz * 8, cudaMemcpyHostToDevice, s);
+  // the host arrays may be reused once this returns: wait for the copies only
+  cudaEvent_t copied = nullptr;
+  if (e == cudaSuccess)
+    e = cudaEventCreateWithFlags(&copied, cudaEventDisableTiming);
+  if (e == cudaSuccess)
+    e = cudaEventRecord(copied, s);
   if (e == cudaSuccess)
     e = cudaMemsetAsync(cnt, 0, sz_rpT, s);
   if (e == cudaSuccess && nnz) {
@@ -413,7 +438,7 @@ int krans_csr_create(krans_ctx *ctx, int64_t m, int64_t n, int64_t nnz, const in
     row_sort_kernel<<<grid_for(ctx, n * 32), 256, 0, s>>>(n, A->rpT, perm, tmp);
     row_of_kernel<<<grid_for(ctx, m * 32), 256, 0, s>>>(m, A->rp, rowof);
     gather_t_kernel<<<g, 256, 0, s>>>(nnz, perm, rowof, A->v, A->ciT, A->vT);
-    if (flags & KRANS_CSR_FP32) {
+    if (f32) {
       to_f32_kernel<<<g, 256, 0, s>>>(nnz, A->v, A->v32);
       to_f32_kernel<<<g, 256, 0, s>>>(nnz, A->vT, A->vT32);
     }
@@ -422,13 +447,19 @@ int krans_csr_create(krans_ctx *ctx, int64_t m, int64_t n, int64_t nnz, const in
   }
   if (e == cudaSuccess)
     e = cudaGetLastError();
-  if (e == cudaSuccess)
-    e = cudaStreamSynchronize(s);
-  dev_free(ctx, cnt, sz_rpT);
-  dev_free(ctx, perm, sz_ci);
-  dev_free(ctx, tmp, sz_ci);
-  dev_free(ctx, rowof, sz_ci);
+  if (scratch) {
+    const cudaError_t ef = cudaFreeAsync(scratch, s);
+    if (e == cudaSuccess)
+      e = ef;
+  }
+  if (copied) {
+    const cudaError_t es = cudaEventSynchronize(copied);
+    if (e == cudaSuccess)
+      e = es;
+    cudaEventDestroy(copied);
+  }
   if (e != cudaSuccess) {
+    cudaStreamSynchronize(s);
     rc = cuda_fail(e, "krans_csr_create", __FILE__, __LINE__);
     krans_csr_destroy(A);
     return rc;
@@ -437,21 +468,8 @@ int krans_csr_create(krans_ctx *ctx, int64_t m, int64_t n, int64_t nnz, const in
   A->lanesT = pick_lanes(n, nnz);
   // uniform row lengths (e.g. incidence and difference operators) let the
   // SpMV skip the row pointers and use vector loads
-  {
-    const int64_t L = m > 0 ? (int64_t)(row_ptr[1] - row_ptr[0]) : 0;
-    bool uni = m > 0 && L > 0 && L <= 8;
-    for (int64_t i = 0; uni && i < m; i++)
-      uni = (int64_t)(row_ptr[i + 1] - row_ptr[i]) == L;
-    A->ulen = uni ? (int32_t)L : 0;
-    std::vector<int32_t> cc((size_t)n, 0);
-    for (int64_t k = 0; k < nnz; k++)
-      cc[(size_t)col_idx[k]]++;
-    const int32_t LT = n > 0 ? cc[0] : 0;
-    bool uniT = n > 0 && LT > 0 && LT <= 8;
-    for (int64_t j = 0; uniT && j < n; j++)
-      uniT = cc[(size_t)j] == LT;
-    A->ulenT = uniT ? LT : 0;
-  }
+  A->ulen = uni ? (int32_t)L : 0;
+  A->ulenT = uniT ? LT : 0;
   *out = A;
   return KRANS_OK;
 }
@@ -459,17 +477,7 @@ int krans_csr_create(krans_ctx *ctx, int64_t m, int64_t n, int64_t nnz, const in
 int krans_csr_destroy(krans_mat *A) {
   if (!A)
     return KRANS_OK;
-  krans_ctx *c = A->ctx;
-  const size_t sz_rp = (size_t)(A->m + 1) * 4, sz_rpT = (size_t)(A->n + 1) * 4;
-  const size_t sz_ci = (size_t)std::max<int64_t>(A->nnz, 1) * 4, sz_v = (size_t)std::max<int64_t>(A->nnz, 1) * 8;
-  dev_free(c, A->rp, sz_rp);
-  dev_free(c, A->ci, sz_ci);
-  dev_free(c, A->v, sz_v);
-  dev_free(c, A->rpT, sz_rpT);
-  dev_free(c, A->ciT, sz_ci);
-  dev_free(c, A->vT, sz_v);
-  dev_free(c, A->v32, sz_ci);
-  dev_free(c, A->vT32, sz_ci);
+  dev_free(A->ctx, A->base, A->bytes);
   delete A;
   return KRANS_OK;
 }

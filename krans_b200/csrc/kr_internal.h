@@ -74,6 +74,7 @@ struct krans_mat {
   float *v32 = nullptr, *vT32 = nullptr;
   int lanes = 1, lanesT = 1;
   int32_t ulen = 0, ulenT = 0; // uniform row length of A / A^T (0 = not uniform)
+  char *base = nullptr;         // one device allocation holding every stored array
   size_t bytes = 0;
 };
 
