@@ -131,3 +131,25 @@ def test_server_cancel_and_budget(ctx):
     st, res = tiny.poll(t)
     assert st == "failed" and res.status == -4  # KRANS_ERR_OUT_OF_MEMORY
     tiny.close()
+
+
+def test_size_classes_and_pair_launch(ctx, oracle):
+    """A batch with single-block (m + n < 16384), 2-block-cluster (< 120000)
+    and 8-block-cluster requests: all converge, and a mid-size request gives
+    bit-identical results alone and in the mix (its team kind depends only on
+    its size)."""
+    from krans_b200.serving import solve_batch
+    insts = [G.shift_operator(3000, 2, 0.5), G.graph_incidence(2500, 3, 6.0, seed=1),
+             G.shift_operator(20000, 3, 0.6), G.graph_incidence(12000, 4, 6.0, seed=2),
+             G.shift_operator(70000, 2, 0.7), G.graph_incidence(40000, 2, 6.0, seed=3)]
+    mix = make_requests(ctx, insts, 1)
+    solve_batch(ctx, mix)
+    for inst, rq in zip(insts, mix):
+        r = rq.result
+        assert r.status == 0 and r.converged_to_target and r.n_right == inst.k
+        assert r.max_residual <= 1e-12 * norm_lower_bound(inst.A)
+        assert oracle.subspace_dist(inst.kernel, rq.basis()) <= 1e-10
+    for i in (2, 3):
+        alone = make_requests(ctx, [insts[i]], 1, seed0=11 + i)
+        solve_batch(ctx, alone)
+        np.testing.assert_array_equal(alone[0].basis(), mix[i].basis())
