@@ -62,6 +62,14 @@ int krans_ctx_memory_in_use(const krans_ctx *ctx, size_t *bytes);
 /* Number of SMs of the context's device. */
 int krans_ctx_sm_count(const krans_ctx *ctx, int *sms);
 
+/* Self-test of failure detection (no reference counterpart): runs a two-block
+ * cooperative kernel whose first block waits at a grid barrier that the second
+ * never reaches. The wait is bounded by timeout_ms (the solvers' barriers use
+ * 8 s); when it runs out the kernel returns with KRANS_ERR_TIMEOUT in
+ * *status_out (0 would mean the wait did not give up), *elapsed_ms gets the
+ * kernel's device time, and the context stays usable. */
+int krans_selftest_barrier_timeout(krans_ctx *ctx, double timeout_ms, int *status_out, double *elapsed_ms);
+
 /* ---- CSR matrix: MatrixInterface (rows, cols, multiply, multiply_transpose) --
  * Replaces EigenSparseMatrixAdapter(A), which owns A and a cached transpose
  * (include/krans/adapters/eigen/EigenSparseMatrixAdapter.hpp:20-24,56).

@@ -121,6 +121,7 @@ SIGNATURES = {
     "krans_ctx_sm_count": [P, C.POINTER(I)],
     "krans_csr_create": [P, I64, I64, I64, P, P, P, I, PP],
     "krans_csr_destroy": [P],
+    "krans_selftest_barrier_timeout": [P, D, C.POINTER(I), C.POINTER(D)],
     "krans_csr_read_host": [C.c_char_p, I, C.POINTER(I64), C.POINTER(I64), C.POINTER(I64),
                             C.POINTER(C.POINTER(C.c_int32)), C.POINTER(C.POINTER(C.c_int32)),
                             C.POINTER(C.POINTER(C.c_double))],

@@ -341,6 +341,78 @@ int krans_ctx_sm_count(const krans_ctx *ctx, int *sms) {
 // ---------------------------------------------------------------------------
 // CSR
 // ---------------------------------------------------------------------------
+// ---------------------------------------------------------------------------
+// Self-test of the bounded grid barrier: block 0 waits at a barrier that
+// block 1 never reaches (it returns at once), so the wait must run out after
+// the state's timeout and leave KRANS_ERR_TIMEOUT in the status word.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(64) barrier_timeout_probe_kernel(GridBarrierState *gb, int *status,
+                                                                   double *gpart) {
+  __shared__ TeamShared sh;
+  if (blockIdx.x != 0)
+    return;
+  TeamGrid tm{&sh, status, gb, gpart, 0, 0};
+  tm.sync();
+}
+
+extern "C" int krans_selftest_barrier_timeout(krans_ctx *ctx, double timeout_ms, int *status_out,
+                                              double *elapsed_ms) {
+  KR_CHECK_ARG(ctx && status_out, "krans_selftest_barrier_timeout: NULL argument");
+  KR_CHECK_ARG(timeout_ms > 0.0 && timeout_ms <= 10000.0,
+               "krans_selftest_barrier_timeout: timeout_ms must be in (0, 10000]");
+  KR_CUDA(cudaSetDevice(ctx->device));
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  struct Probe {
+    GridBarrierState gb;
+    int status;
+    int pad;
+    double gpart[2 * 2 * KR_RED_K];
+  };
+  Probe *d = nullptr;
+  int rc = dev_alloc(ctx, (void **)&d, sizeof(Probe));
+  if (rc != KRANS_OK)
+    return rc;
+  Probe h;
+  memset(&h, 0, sizeof h);
+  h.gb.timeout_ns = (uint64_t)(timeout_ms * 1e6);
+  cudaStream_t s = ctx->stream;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  cudaError_t e = cudaMemcpyAsync(d, &h, sizeof h, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess)
+    e = cudaEventCreate(&e0);
+  if (e == cudaSuccess)
+    e = cudaEventCreate(&e1);
+  if (e == cudaSuccess)
+    e = cudaEventRecord(e0, s);
+  if (e == cudaSuccess) {
+    GridBarrierState *gb = &d->gb;
+    int *st = &d->status;
+    double *gp = d->gpart;
+    void *args[] = {(void *)&gb, (void *)&st, (void *)&gp};
+    e = cudaLaunchCooperativeKernel((const void *)barrier_timeout_probe_kernel, dim3(2), dim3(64), args, 0, s);
+  }
+  if (e == cudaSuccess)
+    e = cudaEventRecord(e1, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(&h, d, sizeof h, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess)
+    e = cudaStreamSynchronize(s);
+  float ms = 0.f;
+  if (e == cudaSuccess)
+    e = cudaEventElapsedTime(&ms, e0, e1);
+  if (e0)
+    cudaEventDestroy(e0);
+  if (e1)
+    cudaEventDestroy(e1);
+  dev_free(ctx, d, sizeof(Probe));
+  if (e != cudaSuccess)
+    return cuda_fail(e, "krans_selftest_barrier_timeout", __FILE__, __LINE__);
+  *status_out = h.status;
+  if (elapsed_ms)
+    *elapsed_ms = ms;
+  return KRANS_OK;
+}
+
 int krans_csr_create(krans_ctx *ctx, int64_t m, int64_t n, int64_t nnz, const int32_t *row_ptr,
                      const int32_t *col_idx, const double *values, int flags, krans_mat **out) {
   KR_CHECK_ARG(ctx && out, "krans_csr_create: NULL argument");

@@ -145,10 +145,11 @@ struct TeamGrid {
           atomicAdd(&gb->gen, 1u);
         } else {
           const uint64_t t0 = globaltimer_ns();
+          const uint64_t limit = gb->timeout_ns ? gb->timeout_ns : kBarrierTimeoutNs;
           while (*vgen == g) {
             if (*verr != 0)
               break;
-            if (globaltimer_ns() - t0 > kBarrierTimeoutNs) {
+            if (globaltimer_ns() - t0 > limit) {
               atomicCAS(&gb->error, 0, KRANS_ERR_TIMEOUT);
               atomicCAS(err, 0, KRANS_ERR_TIMEOUT);
               break;

@@ -21,6 +21,7 @@ struct GridBarrierState {
   unsigned int gen;
   int error; // sticky: once set, barriers return at once and solvers unwind
   int pad;
+  uint64_t timeout_ns; // longest wait at one barrier; 0 = the default (kBarrierTimeoutNs)
 };
 
 // State of one factory stream. Layout of the MT part equals the CPU oracle's.

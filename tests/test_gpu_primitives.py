@@ -132,3 +132,22 @@ def test_philox_stream(ctx):
     assert not np.array_equal(a, b)
     g = kb.CudaVectorFactory(ctx, 100000, seed=7, mode="philox")
     np.testing.assert_array_equal(g.create_random().data(), a)
+
+
+def test_bounded_grid_barrier_wait_runs_out(ctx):
+    """Failure detection without a GPU fault: a grid barrier that one block
+    never reaches gives up after its bound with KRANS_ERR_TIMEOUT, and the
+    context keeps working (a solve right after succeeds)."""
+    import ctypes as C
+    import krans_b200 as kb
+    from krans_b200 import _capi as K
+    from krans_b200 import generators as G
+    st, ms = C.c_int(0), C.c_double(0.0)
+    K.check(ctx.lib.krans_selftest_barrier_timeout(ctx.h, 300.0, C.byref(st), C.byref(ms)))
+    assert st.value == K.KRANS_ERR_TIMEOUT
+    assert 300.0 <= ms.value < 3000.0
+    inst = G.shift_operator(1000, 3, 0.5)
+    M = kb.CudaCsrMatrixAdapter.from_scipy(ctx, inst.A)
+    R = kb.find_nullspace_cyclic_lanczos_ex(M, kb.CudaVectorFactory(ctx, 1000, seed=42),
+                                            kb.CyclicLanczosOptions(k=3))
+    assert R.converged_to_target and len(R.right_null) == 3
