@@ -217,7 +217,8 @@ typedef struct krans_cyclic_opts {
   int32_t team;              /* KRANS_TEAM_AUTO */
   int32_t precond_aat;       /* KRANS_PRECOND_NONE: the device form of precond_AAt */
   int32_t precond_steps;     /* steps of KRANS_PRECOND_SD (8) */
-  int32_t polish_block;      /* 0: polish candidates one by one (the reference's order);
+  int32_t polish_block;      /* (ignored when precond_aat is set)
+                                0: polish candidates one by one (the reference's order);
                                 1: project up to 8 candidates of a restart with one block CG
                                 (matrix read once per iteration for all of them) */
 } krans_cyclic_opts;

@@ -293,6 +293,13 @@ class Precision(enum.IntEnum):
     MIXED = K.KRANS_PREC_MIXED
 
 
+class Precond(enum.IntEnum):
+    """Device preconditioners (the device form of precond_AAt / M_inv)."""
+    NONE = K.KRANS_PRECOND_NONE
+    JACOBI = K.KRANS_PRECOND_JACOBI
+    SD = K.KRANS_PRECOND_SD
+
+
 @dataclass
 class CyclicLanczosOptions:
     k: int = 1
@@ -319,7 +326,7 @@ class CyclicLanczosOptions:
     # engine knobs (no reference counterpart)
     precision: Precision = Precision.FP64
     team: int = K.KRANS_TEAM_AUTO
-    precond_aat: int = K.KRANS_PRECOND_NONE  # device form of precond_AAt (JACOBI or SD)
+    precond_aat: Precond = Precond.NONE  # device form of precond_AAt (Precond.JACOBI or Precond.SD)
     precond_steps: int = 8                   # steps of the SD preconditioner
     polish_block: int = 0  # 1: block CG polish of up to 8 candidates at once
 
@@ -369,7 +376,7 @@ class LOBPCGOptions:
     progress_every: int = 100
     precision: Precision = Precision.FP64
     team: int = K.KRANS_TEAM_AUTO
-    precond_normal: int = K.KRANS_PRECOND_NONE  # device form of M_inv (JACOBI or SD)
+    precond_normal: Precond = Precond.NONE  # device form of M_inv (Precond.JACOBI or Precond.SD)
     precond_steps: int = 6                      # steps of the SD preconditioner
 
     def to_c(self) -> K.LobpcgOpts:

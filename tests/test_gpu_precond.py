@@ -50,7 +50,7 @@ def test_precond_matches_oracle(ctx, oracle, kind):
     import krans_b200 as kb
     A, K = weighted_incidence(3000, 3, 7)
     A = A.tocsr()
-    pk = kb._capi.KRANS_PRECOND_JACOBI if kind == "jacobi" else kb._capi.KRANS_PRECOND_SD
+    pk = kb.Precond.JACOBI if kind == "jacobi" else kb.Precond.SD
     fn = jacobi_fn(A) if kind == "jacobi" else sd_fn(A, 8)
     opts = dict(k=3, cg_maxit=200)
     M = kb.CudaCsrMatrixAdapter.from_scipy(ctx, A)
@@ -80,7 +80,7 @@ def test_reference_mat2_with_sd_preconditioner(ctx, oracle):
         k=nul, ncv=max(nul + 80, 128), max_restarts=400, projector_passes=2, cg_maxit=200, cg_rel_tol=1e-10,
         prescreen_factor=4.0, stagnation_restarts=0, tol_abs=1e-12, tol_rel=1e-10, nullity_known=nul,
         rank_known=A.shape[1] - nul, initial_right_space=[vf.create_random_of_size(A.shape[1])],
-        precond_aat=kb._capi.KRANS_PRECOND_SD, precond_steps=8)
+        precond_aat=kb.Precond.SD, precond_steps=8)
     R = kb.find_nullspace_cyclic_lanczos_ex(M, vf, opt)
     U = kb.basis_to_numpy(R.right_null)
     # the reference test's checks: every ||A u|| within the acceptance
@@ -127,7 +127,7 @@ def test_lobpcg_reference_mat1_with_sd_preconditioner(ctx, oracle):
     init = [vf.create_random_of_size(A.shape[1]) for _ in range(2)]
     R = kb.find_nullspace_lobpcg_ex(M, vf, kb.LOBPCGOptions(
         nev=5, block_size=12, max_iters=500, tol_abs=1e-12, tol_rel=1e-10, nullity_known=5, rank_known=100,
-        initial_block=init, precond_normal=kb._capi.KRANS_PRECOND_SD, precond_steps=6))
+        initial_block=init, precond_normal=kb.Precond.SD, precond_steps=6))
     U = kb.basis_to_numpy(R.right_null)
     assert U.shape[0] == nul
     assert np.all(np.abs(np.linalg.norm(U, axis=1) - 1) <= 1e-10)
@@ -145,9 +145,9 @@ def test_lobpcg_precond_matches_oracle(ctx, oracle, kind):
     if kind == "jacobi":
         d = np.asarray(A.multiply(A).sum(axis=0)).ravel()
         dinv = np.where(d > 0, 1.0 / np.where(d > 0, d, 1.0), 1.0)
-        fn, pk = (lambda r: dinv * r), kb._capi.KRANS_PRECOND_JACOBI
+        fn, pk = (lambda r: dinv * r), kb.Precond.JACOBI
     else:
-        fn, pk = sd_normal_fn(A, 6), kb._capi.KRANS_PRECOND_SD
+        fn, pk = sd_normal_fn(A, 6), kb.Precond.SD
     opts = dict(nev=4, block_size=8, max_iters=800)
     M = kb.CudaCsrMatrixAdapter.from_scipy(ctx, A)
     R = kb.find_nullspace_lobpcg_ex(M, kb.CudaVectorFactory(ctx, A.shape[1], seed=9),
