@@ -1,6 +1,8 @@
 // Tall-skinny products of the block solver:
-//   team_gemm_tn_tiled: C = A^T B (Gram matrices S = Z^T Z, G = Z^T (AZ),
-//                       Cholesky QR, projections), FP64 tensor cores
+//   team_gemm_tn:       C = A^T B (Gram matrices S = Z^T Z, G = Z^T (AZ),
+//                       Cholesky QR, projections), FP64 tensor cores: tiled
+//                       with shared-memory panels for long, wide products,
+//                       one warp per output tile otherwise
 //   team_combine_sub:   X -= S C
 //   team_combine:       out = Z * Y[roff:roff+zc, 0:q] (n x q)
 // Sums run in a fixed order that depends only on the team size, so results
@@ -134,6 +136,77 @@ KR_DEV void team_gemm_tn_tiled(Team &tm, int64_t n, const double *A, int a, cons
     C[e] = s;
   }
   tm.sync();
+}
+
+// C = A^T B for tall-skinny A (n x a) and B (n x b), column-major with
+// leading dim ld; C is a x b with leading dim a. DMMA 8x8 tiles, one warp per
+// tile; each block reduces its fixed row range into a private partial, then
+// the partials are summed in block order (deterministic for a team size).
+template <class Team>
+KR_DEV void team_gemm_tn_direct(Team &tm, int64_t n, const double *A, int a, const double *B, int b, int64_t ld,
+                         double *C, double *part) {
+  const int ta = (a + 7) / 8, tb = (b + 7) / 8, ntiles = ta * tb;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int ncta = tm.ncta(), rank = tm.cta_rank();
+  const int64_t per = (n + ncta - 1) / ncta;
+  const int64_t r0 = imin64((int64_t)rank * per, n), r1 = imin64(r0 + per, n);
+  double *my = part + (size_t)rank * a * b;
+  for (int t = wid; t < ntiles; t += nw) {
+    const int bi = t % ta, bj = t / ta;
+    const int ia = bi * 8 + (lane >> 2), jb = bj * 8 + (lane >> 2);
+    const bool va = ia < a, vb = jb < b;
+    const double *pa = A + (int64_t)(va ? ia : 0) * ld;
+    const double *pb = B + (int64_t)(vb ? jb : 0) * ld;
+    double c0 = 0.0, c1 = 0.0, e0 = 0.0, e1 = 0.0;
+    int64_t base = r0;
+    for (; base + 8 <= r1; base += 8) { // two independent accumulators
+      const int64_t r = base + (lane & 3);
+      const double x0 = va ? pa[r] : 0.0, y0 = vb ? pb[r] : 0.0;
+      const double x1 = va ? pa[r + 4] : 0.0, y1 = vb ? pb[r + 4] : 0.0;
+      dmma_8x8x4(c0, c1, x0, y0);
+      dmma_8x8x4(e0, e1, x1, y1);
+    }
+    for (; base < r1; base += 4) {
+      const int64_t r = base + (lane & 3);
+      const bool in = r < r1;
+      const double x0 = (in && va) ? pa[r] : 0.0, y0 = (in && vb) ? pb[r] : 0.0;
+      dmma_8x8x4(c0, c1, x0, y0);
+    }
+    c0 += e0;
+    c1 += e1;
+    const int ci = bi * 8 + (lane >> 2), cj = bj * 8 + 2 * (lane & 3);
+    if (ci < a) {
+      if (cj < b)
+        my[ci + (size_t)cj * a] = c0;
+      if (cj + 1 < b)
+        my[ci + (size_t)(cj + 1) * a] = c1;
+    }
+  }
+  tm.sync();
+  const int64_t nt = tm.nthreads();
+  for (int64_t e = tm.tid(); e < (int64_t)a * b; e += nt) {
+    double s = 0.0;
+    for (int r = 0; r < ncta; r++)
+      s += __ldcg(part + (size_t)r * a * b + e);
+    C[e] = s;
+  }
+  tm.sync();
+}
+
+
+// C = A^T B: the tiled kernel for long products with wide blocks, where the
+// shared-memory panels pay off; the direct one (one warp per 8 x 8 tile,
+// operands straight from global memory) for short or narrow ones, where
+// streaming full 64-column panels 16 rows at a time through one block costs
+// more than it saves (measured: a 1000-row LOBPCG with 3-column blocks ran
+// 3.3x slower tiled). `part` must suit both (see each).
+template <class Team>
+KR_DEV void team_gemm_tn(Team &tm, int64_t n, const double *A, int a, const double *B, int b, int64_t ld,
+                         double *C, double *part) {
+  if (n >= 131072 && (a >= 32 || b >= 32))
+    team_gemm_tn_tiled(tm, n, A, a, B, b, ld, C, part);
+  else
+    team_gemm_tn_direct(tm, n, A, a, B, b, ld, C, part);
 }
 
 // X[:, i] -= sum_j S[:, j] * Cc(j, i) for i < k, j < ns (X, S column-major

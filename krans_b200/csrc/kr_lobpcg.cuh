@@ -236,7 +236,7 @@ template <class Team> struct LobpcgSolver {
     if (k <= 0)
       return true;
     if (nb > 0) {
-      team_gemm_tn_tiled(tm, n, basis, (int)nb, Xb, (int)k, ldn, d.Cm, d.gram_part);
+      team_gemm_tn(tm, n, basis, (int)nb, Xb, (int)k, ldn, d.Cm, d.gram_part);
       team_combine_sub(tm, n, basis, ldn, (int)nb, d.Cm, (int)nb, (int)k, Xb);
       tm.sync();
       gram_flops += 4.0 * (double)n * nb * k;
@@ -335,7 +335,7 @@ template <class Team> struct LobpcgSolver {
 
   // one Cholesky-QR round: out = V chol(V^T V)^-T (V unchanged)
   __device__ __noinline__ bool cholqr_round(const double *V, int64_t k, double tol, double *out) {
-    team_gemm_tn_tiled(tm, n, V, (int)k, V, (int)k, ldn, d.Sj, d.gram_part);
+    team_gemm_tn(tm, n, V, (int)k, V, (int)k, ldn, d.Sj, d.gram_part);
     gram_flops += 2.0 * (double)n * k * k;
     c.bytes += 8.0 * n * k;
     if (!chol_inv_t((int)k, tol))
@@ -376,8 +376,8 @@ template <class Team> struct LobpcgSolver {
 
   __device__ __noinline__ void form_gram(const double *Zb, const double *AZb, int p) {
     const uint64_t t0 = globaltimer_ns();
-    team_gemm_tn_tiled(tm, n, Zb, p, Zb, p, ldn, d.S, d.gram_part);
-    team_gemm_tn_tiled(tm, n, Zb, p, AZb, p, ldn, d.G, d.gram_part);
+    team_gemm_tn(tm, n, Zb, p, Zb, p, ldn, d.S, d.gram_part);
+    team_gemm_tn(tm, n, Zb, p, AZb, p, ldn, d.G, d.gram_part);
     t_ph[1] += globaltimer_ns() - t0;
     gram_flops += 2.0 * 2.0 * (double)n * p * p;
     c.bytes += 2.0 * 8.0 * n * p;
