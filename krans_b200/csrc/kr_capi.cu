@@ -281,7 +281,7 @@ int krans_ctx_create(int device, size_t hbm_budget_bytes, krans_ctx **out) {
   c->cc_minor = prop.minor;
   if (prop.major != 10) {
     delete c;
-    set_error("krans_ctx_create: device %d is sm_%d%d; this build targets sm_100a (B200)", device,
+    set_error("krans_ctx_create: device %d is sm_%d%d; this library targets sm_100a (B200)", device,
               prop.major, prop.minor);
     return KRANS_ERR_RUNTIME;
   }

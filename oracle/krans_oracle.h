@@ -3,7 +3,7 @@
  * null-space solvers (Deep-SANE/krans). TEST INFRASTRUCTURE ONLY.
  *
  * Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg may
- * load this library, and there only as the checker / CPU baseline. The
+ * load this library, and there only as the reference result / CPU baseline. The
  * product path (krans_b200/, libkrans_cuda.so) never links or calls it.
  *
  * What it restates (reference file:line):

@@ -1,7 +1,7 @@
 """Regenerate the committed golden fixtures under tests/golden/.
 
 Run in the development container (it reads the reference checkout and needs
-g++); the GPU box only reads the committed outputs:
+g++); GPU test runs only read the committed outputs:
 
     python tests/golden/make_golden.py /path/to/reference
 

@@ -1,6 +1,6 @@
 """bench.py's reference arm runs the CPU oracle only, so its JSON contract is
 checked here on a tiny sample: same metric, unit and config as the GPU arm,
-plus the reference keys the driver reads."""
+plus the keys of the reference arm."""
 import json
 import os
 import subprocess

@@ -1,5 +1,5 @@
 """Pins the CPU oracle against the reference's own known answers and golden
-vectors (CPU only). The oracle is the checker for every GPU parity test.
+vectors (CPU only). The oracle is the reference result of every GPU parity test.
 
 Known answers used (reference paths):
   examples/quickstart.cpp:41-66, README.md:74-79   config-1 shift operator
