@@ -3,6 +3,8 @@
 //                       Cholesky QR, projections), FP64 tensor cores: tiled
 //                       with shared-memory panels for long, wide products,
 //                       one warp per output tile otherwise
+//   team_gram2_direct:  S = Z^T Z and G = Z^T (AZ) in one pass (short or
+//                       narrow blocks)
 //   team_combine_sub:   X -= S C
 //   team_combine:       out = Z * Y[roff:roff+zc, 0:q] (n x q)
 // Sums run in a fixed order that depends only on the team size, so results
@@ -189,6 +191,82 @@ KR_DEV void team_gemm_tn_direct(Team &tm, int64_t n, const double *A, int a, con
     for (int r = 0; r < ncta; r++)
       s += __ldcg(part + (size_t)r * a * b + e);
     C[e] = s;
+  }
+  tm.sync();
+}
+
+
+// S = Z^T Z and G = Z^T (AZ) (p x p, both triangles) in one pass, one warp
+// per 8x8 upper tile with DMMA, operands straight from global memory; each
+// block reduces its fixed row range into a private partial (2 p^2 doubles per
+// block in `part`), summed in block order. Used for short or narrow blocks.
+template <class Team>
+KR_DEV void team_gram2_direct(Team &tm, int64_t n, const double *Z, const double *AZ, int64_t ld, int p,
+                       double *S, double *G, double *part) {
+  const int nt8 = (p + 7) / 8;                       // 8x8 tiles per dimension
+  const int ntiles = nt8 * (nt8 + 1) / 2;            // upper triangle incl. diagonal
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int ncta = tm.ncta(), rank = tm.cta_rank();
+  // fixed row range of this block
+  const int64_t per = (n + ncta - 1) / ncta;
+  const int64_t r0 = imin64((int64_t)rank * per, n), r1 = imin64(r0 + per, n);
+  double *myS = part + (size_t)rank * 2 * p * p;
+  double *myG = myS + (size_t)p * p;
+  // a warp owns one 8x8 tile at a time; the MMA lane layout of m8n8k4:
+  // A(row=lane>>2, k=lane&3), B(k=lane&3, col=lane>>2), C rows lane>>2,
+  // cols 2*(lane&3) and 2*(lane&3)+1.
+  for (int t = wid; t < ntiles; t += nw) {
+    // decode upper-triangular tile index t -> (bi <= bj)
+    int bi = 0, rem = t;
+    while (rem >= nt8 - bi) {
+      rem -= nt8 - bi;
+      bi++;
+    }
+    const int bj = bi + rem;
+    const int ia = bi * 8 + (lane >> 2), jb = bj * 8 + (lane >> 2);
+    const bool va = ia < p, vb = jb < p;
+    const double *za = Z + (int64_t)(va ? ia : 0) * ld;
+    const double *zb = Z + (int64_t)(vb ? jb : 0) * ld;
+    const double *azb = AZ + (int64_t)(vb ? jb : 0) * ld;
+    double s0 = 0.0, s1 = 0.0, g0 = 0.0, g1 = 0.0;
+    for (int64_t base = r0; base < r1; base += 4) { // warp-uniform trip count
+      const int64_t r = base + (lane & 3);
+      const bool in = r < r1;
+      const double a = (in && va) ? za[r] : 0.0;
+      const double b = (in && vb) ? zb[r] : 0.0;
+      const double ab = (in && vb) ? azb[r] : 0.0;
+      dmma_8x8x4(s0, s1, a, b);
+      dmma_8x8x4(g0, g1, a, ab);
+    }
+    const int ci = bi * 8 + (lane >> 2), cj = bj * 8 + 2 * (lane & 3);
+    if (ci < p) {
+      if (cj < p) {
+        myS[ci + (size_t)cj * p] = s0;
+        myG[ci + (size_t)cj * p] = g0;
+      }
+      if (cj + 1 < p) {
+        myS[ci + (size_t)(cj + 1) * p] = s1;
+        myG[ci + (size_t)(cj + 1) * p] = g1;
+      }
+    }
+  }
+  tm.sync();
+  // sum the block partials in block order; fill both triangles
+  const int64_t nt = tm.nthreads();
+  for (int64_t e = tm.tid(); e < (int64_t)p * p; e += nt) {
+    const int j = (int)(e / p), i = (int)(e % p);
+    if (i > j)
+      continue;
+    double s = 0.0, g = 0.0;
+    for (int b = 0; b < ncta; b++) {
+      const double *ps = part + (size_t)b * 2 * p * p;
+      s += __ldcg(ps + e);
+      g += __ldcg(ps + (size_t)p * p + e);
+    }
+    S[i + (size_t)j * p] = s;
+    S[j + (size_t)i * p] = s;
+    G[i + (size_t)j * p] = g;
+    G[j + (size_t)i * p] = g;
   }
   tm.sync();
 }

@@ -376,8 +376,12 @@ template <class Team> struct LobpcgSolver {
 
   __device__ __noinline__ void form_gram(const double *Zb, const double *AZb, int p) {
     const uint64_t t0 = globaltimer_ns();
-    team_gemm_tn(tm, n, Zb, p, Zb, p, ldn, d.S, d.gram_part);
-    team_gemm_tn(tm, n, Zb, p, AZb, p, ldn, d.G, d.gram_part);
+    if (n >= 131072 && p >= 32) {
+      team_gemm_tn(tm, n, Zb, p, Zb, p, ldn, d.S, d.gram_part);
+      team_gemm_tn(tm, n, Zb, p, AZb, p, ldn, d.G, d.gram_part);
+    } else {
+      team_gram2_direct(tm, n, Zb, AZb, ldn, p, d.S, d.G, d.gram_part); // both in one pass
+    }
     t_ph[1] += globaltimer_ns() - t0;
     gram_flops += 2.0 * 2.0 * (double)n * p * p;
     c.bytes += 2.0 * 8.0 * n * p;
