@@ -129,9 +129,10 @@ def measured_peak():
     return 6650.0, "fallback"
 
 
-# DRAM bytes (read + write) per algorithmic byte of the batched launch, from
-# one ncu capture of a 64-instance batch (larger than L2):
-# profiles/batched_launch_list_batch256.md. `traffic` scales it to this launch.
+# DRAM bytes (read + write) per algorithmic byte of the batched launch, taken
+# from one ncu capture (dram__bytes_read.sum + dram__bytes_write.sum) of the
+# batched kernel on a 64-instance batch of this workload, whose matrices
+# exceed L2. `traffic` scales it to this launch.
 DRAM_PER_ALGO_BYTE = 1.607e12 / 3.966e12
 
 
@@ -609,6 +610,98 @@ def run_planted(args):
     return 0
 
 
+def spmv_bytes(rows, cols, nnz, w, wx=8, wy=8):
+    """Algorithmic bytes of one CSR SpMV: row pointers, (column, value) pairs,
+    x once, y once (int32 indices)."""
+    return 4.0 * (rows + 1) + nnz * (w + 4.0) + cols * wx + rows * wy
+
+
+class StreamTimer:
+    """CUDA events on the library context's own stream (the stream the
+    kernels are launched on)."""
+
+    def __init__(self, ctx):
+        import torch
+        self.torch = torch
+        self.stream = torch.cuda.ExternalStream(ctx.stream_ptr(), device=f"cuda:{ctx.device}")
+
+    def time(self, fn, reps):
+        t = self.torch
+        e0, e1 = t.cuda.Event(enable_timing=True), t.cuda.Event(enable_timing=True)
+        t.cuda.synchronize()
+        e0.record(self.stream)
+        for _ in range(reps):
+            fn()
+        e1.record(self.stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+
+def run_spmv(args):
+    """Standalone SpMV / SpM^T V on the large matrices of the LOBPCG and
+    planted-kernel workloads (graph incidence 64 x 2^s vertices, mean degree
+    8; planted kernel m = 3e6 / 2^(16-s)), FP64 and FP32 values, A and the
+    stored transpose, through the C ABI (krans_spmv_ex). Each case reports
+    algorithmic GB/s (row pointers + (column, value) pairs + x once + y once)
+    against the measured HBM copy bandwidth, for the automatic kernel and the
+    lanes-per-row form the solver teams use."""
+    import krans_b200 as kb
+    from krans_b200 import _capi as K
+    from krans_b200 import generators as G
+    ctx = kb.Context(0)
+    timer = StreamTimer(ctx)
+    peak, peak_kind = measured_peak()
+    div = 1 << max(0, 16 - args.scale)
+    mats = {
+        "incidence": G.graph_incidence(64 << args.scale, 64, 8.0, seed=1, kernel=False).A,
+        "planted": G.planted_kernel(3_000_000 // div, 2_000_000 // div, 32, seed=1, kernel=False).A,
+    }
+    rng = np.random.default_rng(5)
+    cases = {}
+
+    def measure():
+        for name, A in mats.items():
+            M = kb.CudaCsrMatrixAdapter.from_scipy(ctx, A, fp32=True)
+            for trans in (0, 1):
+                rows, cols = (A.shape[1], A.shape[0]) if trans else A.shape
+                x = kb.CudaVectorAdapter.from_numpy(ctx, rng.standard_normal(cols))
+                y = kb.CudaVectorAdapter(ctx, rows)
+                ref = (A.T @ x.data()) if trans else (A @ x.data())
+                for prec, w in ((K.KRANS_PREC_FP64, 8), (K.KRANS_PREC_MIXED, 4)):
+                    for kern in (K.KRANS_SPMV_AUTO, K.KRANS_SPMV_LANES):
+                        M.set_spmv_tuning(trans, kern)
+                        fn = (lambda: M.multiply_transpose(x, y, prec)) if trans else (lambda: M.multiply(x, y, prec))
+                        for _ in range(max(3, args.warmup)):
+                            fn()
+                        ms = timer.time(fn, max(1, args.steps))
+                        err = float(np.max(np.abs(y.data() - ref)) / max(1e-300, np.max(np.abs(ref))))
+                        gbs = spmv_bytes(rows, cols, A.nnz, w) / (ms * 1e-3) / 1e9
+                        key = f"{name}_{'AT' if trans else 'A'}_{'f64' if w == 8 else 'f32'}_" \
+                              f"{'auto' if kern == K.KRANS_SPMV_AUTO else 'lanes'}"
+                        cases[key] = {"rows": rows, "cols": cols, "nnz": int(A.nnz), "us": ms * 1e3,
+                                      "GBps": gbs, "frac": gbs / peak, "max_rel_err_vs_scipy": err}
+                    M.set_spmv_tuning(trans, K.KRANS_SPMV_AUTO)
+            del M
+    _, clocks = _clocked(measure)
+    auto = {k: v for k, v in cases.items() if k.endswith("_auto")}
+    worst = min(auto.values(), key=lambda v: v["frac"])
+    line = {
+        "metric": "standalone SpMV / SpM^T V achieved GB/s (algorithmic bytes / kernel time)",
+        "value": worst["GBps"], "unit": "GB/s", "higher_is_better": True, "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": worst["us"] / 1e3, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64 and f32 values (f64 x, y)", "data": "synthetic",
+        "config": {"workload": f"graph incidence 64 x 2^{args.scale} vertices (mean degree 8) and planted kernel "
+                               f"m={3_000_000 // div}, n-k={2_000_000 // div}, k=32; A and stored A^T",
+                   "l2": "matrix arrays larger than L2 at full size; x gathered from L2",
+                   "value_is": "the slowest automatic-kernel case"},
+        "roofline": {"bound": "hbm", "achieved": worst["GBps"], "peak": peak, "unit": "GB/s",
+                     "frac": worst["frac"], "peak_kind": peak_kind, "traffic": None},
+        "cases": cases, "clocks": clocks, "gpu_launches": len(cases) * (max(3, args.warmup) + max(1, args.steps)),
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def serving_pool(P, nnz_lo, nnz_hi, seed=7):
     """Request matrices of the serving stream: shift and incidence operators
     (mean degree 6, as in the batched workload), incidence of mean degree 8 and
@@ -734,7 +827,7 @@ def main():
     ap.add_argument("--ref-sample", type=int, default=16)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["batched", "quickstart", "lobpcg", "planted", "serving"],
+    ap.add_argument("--workload", choices=["batched", "quickstart", "lobpcg", "planted", "serving", "spmv"],
                     default="batched")
     ap.add_argument("--scale", type=int, default=16, help="lobpcg/planted: log2 size (16 = full)")
     ap.add_argument("--max-iters", type=int, default=1000)
@@ -755,7 +848,7 @@ def main():
         return run_reference(args)
     if args.workload != "batched":
         return {"quickstart": run_quickstart, "lobpcg": run_lobpcg_incidence, "planted": run_planted,
-                "serving": run_serving}[args.workload](args)
+                "serving": run_serving, "spmv": run_spmv}[args.workload](args)
     return run_ours(args)
 
 

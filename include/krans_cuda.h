@@ -61,6 +61,9 @@ int krans_ctx_synchronize(krans_ctx *ctx);
 int krans_ctx_memory_in_use(const krans_ctx *ctx, size_t *bytes);
 /* Number of SMs of the context's device. */
 int krans_ctx_sm_count(const krans_ctx *ctx, int *sms);
+/* The context's CUDA stream (a cudaStream_t), for callers that order their
+ * own work or timing events against the library's. */
+int krans_ctx_stream(const krans_ctx *ctx, void **stream);
 
 /* Self-test of failure detection (no reference counterpart): runs a two-block
  * cooperative kernel whose first block waits at a grid barrier that the second
@@ -138,18 +141,46 @@ int krans_vec_clone(const krans_vec *src, krans_vec **out);              /* clon
  * Scratch comes from a file-scope device array of KRANS_NOALLOC_DOT_MAX_BLOCKS
  * doubles (128 KiB, held by every GPU that loads the library until exit); n
  * above KRANS_NOALLOC_DOT_MAX_N is rejected with KRANS_ERR_INVALID_ARGUMENT.
- * The first call on a device looks up the array's address (make it before any
- * stream capture). Calls that overlap on the GPU share the array and race. */
+ * The first call under each CUDA context (normally the device's primary
+ * context) looks up the array's address, which is then kept by the context's
+ * unique ID: make that first call before any stream capture, and again after
+ * a cudaDeviceReset. Calls that overlap on the GPU share the array and race. */
 #define KRANS_NOALLOC_DOT_PER_BLOCK 2048LL
 #define KRANS_NOALLOC_DOT_MAX_BLOCKS 16384LL
 #define KRANS_NOALLOC_DOT_MAX_N (KRANS_NOALLOC_DOT_PER_BLOCK * KRANS_NOALLOC_DOT_MAX_BLOCKS)
 int krans_vec_dot_noalloc(const double *x, const double *y, int64_t n, double *result, void *stream);
 
-/* y <- A x (trans = 0) or y <- A^T x (trans = 1): multiply / multiply_transpose.
- * precision: 0 = FP64 values, 1 = FP32 values with FP32 accumulation. */
+/* y <- A x (trans = 0) or y <- A^T x (trans = 1): multiply / multiply_transpose
+ * (EigenSparseMatrixAdapter.hpp:34-57: A_ * x and AT_ * x on the cached
+ * transpose). precision: 0 = FP64 values, 1 = FP32 values with FP32
+ * accumulation. Each row is summed in storage order, one rounded product and
+ * one rounded addition per entry, so the FP64 result equals the reference's
+ * sequential CSR loop bit for bit (kernels KRANS_SPMV_UNIFORM / ROWTILE). */
 int krans_spmv(const krans_mat *A, int trans, const krans_vec *x, krans_vec *y);
 int krans_spmv_ex(const krans_mat *A, int trans, int precision, const krans_vec *x,
                   krans_vec *y);
+
+/* Kernel choice of krans_spmv_ex for one stored operand (no reference
+ * counterpart; the autotuner and the benchmark set it). Zeroed = automatic:
+ * UNIFORM when every row holds exactly 1, 2 or 4 entries, else ROWTILE.
+ *   KRANS_SPMV_ROWTILE  blocks of rows_per_block consecutive rows (0 = from
+ *                       the mean row length); entries streamed in tiles of
+ *                       2048, products staged in shared memory, per-row sums
+ *                       in storage order
+ *   KRANS_SPMV_UNIFORM  one thread per row, vector loads (uniform rows only)
+ *   KRANS_SPMV_LANES    the solver teams' form: a power-of-two group of lanes
+ *                       per row and a warp butterfly (not bit-identical to the
+ *                       sequential loop) */
+#define KRANS_SPMV_AUTO 0
+#define KRANS_SPMV_ROWTILE 1
+#define KRANS_SPMV_UNIFORM 2
+#define KRANS_SPMV_LANES 3
+typedef struct krans_spmv_tuning {
+  int32_t kernel;         /* KRANS_SPMV_* */
+  int32_t rows_per_block; /* ROWTILE: rows per block, 1..2048 (0 = automatic) */
+} krans_spmv_tuning;
+int krans_csr_set_spmv_tuning(krans_mat *A, int trans, const krans_spmv_tuning *t);
+int krans_csr_get_spmv_tuning(const krans_mat *A, int trans, krans_spmv_tuning *t);
 
 /* ---- random vectors: VectorFactory::create_random_of_size ------------------
  * KRANS_RNG_MT19937 reproduces std::mt19937(seed) + std::normal_distribution

@@ -31,6 +31,10 @@ KRANS_FMT_IJA = 2
 KRANS_TEAM_AUTO = 0
 KRANS_TEAM_CTA = 1
 KRANS_TEAM_GRID = 2
+KRANS_SPMV_AUTO = 0
+KRANS_SPMV_ROWTILE = 1
+KRANS_SPMV_UNIFORM = 2
+KRANS_SPMV_LANES = 3
 
 
 class KransError(RuntimeError):
@@ -41,6 +45,10 @@ class KransError(RuntimeError):
 
 class KransInvalidArgument(KransError, ValueError):
     """std::invalid_argument in the reference."""
+
+
+class SpmvTuning(C.Structure):
+    _fields_ = [("kernel", C.c_int32), ("rows_per_block", C.c_int32)]
 
 
 class CyclicOpts(C.Structure):
@@ -119,6 +127,7 @@ SIGNATURES = {
     "krans_ctx_synchronize": [P],
     "krans_ctx_memory_in_use": [P, C.POINTER(C.c_size_t)],
     "krans_ctx_sm_count": [P, C.POINTER(I)],
+    "krans_ctx_stream": [P, PP],
     "krans_csr_create": [P, I64, I64, I64, P, P, P, I, PP],
     "krans_csr_destroy": [P],
     "krans_selftest_barrier_timeout": [P, D, C.POINTER(I), C.POINTER(D)],
@@ -146,6 +155,8 @@ SIGNATURES = {
     "krans_vec_dot_noalloc": [P, P, I64, P, P],
     "krans_spmv": [P, I, P, P],
     "krans_spmv_ex": [P, I, I, P, P],
+    "krans_csr_set_spmv_tuning": [P, I, C.POINTER(SpmvTuning)],
+    "krans_csr_get_spmv_tuning": [P, I, C.POINTER(SpmvTuning)],
     "krans_rng_create": [P, C.c_uint32, I, PP],
     "krans_rng_destroy": [P],
     "krans_rng_normal": [P, P],

@@ -50,6 +50,12 @@ class Context:
         check(self.lib.krans_ctx_sm_count(self.h, C.byref(s)))
         return s.value
 
+    def stream_ptr(self) -> int:
+        """The context's cudaStream_t (for ordering or timing caller work)."""
+        p = C.c_void_p()
+        check(self.lib.krans_ctx_stream(self.h, C.byref(p)))
+        return int(p.value or 0)
+
     def close(self):
         if getattr(self, "h", None):
             self.lib.krans_ctx_destroy(self.h)
@@ -224,6 +230,18 @@ class CudaCsrMatrixAdapter:
     def multiply_transpose(self, x, y, precision: int = K.KRANS_PREC_FP64):
         self._chk(x, y, self.m, self.n, "multiply_transpose")
         check(self.ctx.lib.krans_spmv_ex(self.h, 1, precision, x.h, y.h), "multiply_transpose")
+
+    def set_spmv_tuning(self, trans: bool, kernel: int = K.KRANS_SPMV_AUTO, rows_per_block: int = 0):
+        """Kernel of multiply (trans False) / multiply_transpose (trans True):
+        KRANS_SPMV_AUTO, _ROWTILE (rows_per_block rows per block, 0 = from the
+        mean row length), _UNIFORM (rows of 1, 2 or 4 entries) or _LANES."""
+        t = K.SpmvTuning(kernel, rows_per_block)
+        check(self.ctx.lib.krans_csr_set_spmv_tuning(self.h, int(bool(trans)), C.byref(t)), "set_spmv_tuning")
+
+    def spmv_tuning(self, trans: bool):
+        t = K.SpmvTuning()
+        check(self.ctx.lib.krans_csr_get_spmv_tuning(self.h, int(bool(trans)), C.byref(t)), "spmv_tuning")
+        return int(t.kernel), int(t.rows_per_block)
 
     def __del__(self):
         try:

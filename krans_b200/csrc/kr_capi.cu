@@ -74,25 +74,6 @@ int pick_lanes(int64_t rows, int64_t nnz) {
   return 32;
 }
 
-// ---------------------------------------------------------------------------
-// Flat "team" for standalone kernels: grid-stride loops, no team barriers.
-// ---------------------------------------------------------------------------
-struct TeamFlat {
-  KR_DEV int64_t tid() const { return (int64_t)blockIdx.x * blockDim.x + threadIdx.x; }
-  KR_DEV int64_t nthreads() const { return (int64_t)gridDim.x * blockDim.x; }
-  KR_DEV int64_t warp_id() const { return tid() >> 5; }
-  KR_DEV int64_t nwarps() const { return nthreads() >> 5; }
-};
-
-template <class VT, class XT, class YT>
-__global__ void __launch_bounds__(256) spmv_kernel(int64_t rows, const int32_t *rp, const int32_t *ci,
-                                                   const VT *val, const XT *x, YT *y, int lanes, int32_t ulen) {
-  TeamFlat tm;
-  team_spmv_x(
-      tm, rows, rp, ci, val, [&](int32_t c) { return x[c]; }, lanes, ulen,
-      [&](int64_t i, typename AccOf<VT>::T s) { y[i] = (YT)s; });
-}
-
 // two-stage deterministic reduction: partial per block, then one block sums
 __global__ void __launch_bounds__(256) dot_partial_kernel(int64_t n, const double *x, const double *y,
                                                           double *part) {
@@ -335,6 +316,12 @@ int krans_ctx_memory_in_use(const krans_ctx *ctx, size_t *bytes) {
 int krans_ctx_sm_count(const krans_ctx *ctx, int *sms) {
   KR_CHECK_ARG(ctx && sms, "NULL argument");
   *sms = ctx->sms;
+  return KRANS_OK;
+}
+
+int krans_ctx_stream(const krans_ctx *ctx, void **stream) {
+  KR_CHECK_ARG(ctx && stream, "NULL argument");
+  *stream = (void *)ctx->stream;
   return KRANS_OK;
 }
 
@@ -718,19 +705,30 @@ int krans_spmv_ex(const krans_mat *A, int trans, int precision, const krans_vec 
   KR_CHECK_ARG(A && x && y, "krans_spmv: NULL argument");
   const int64_t rows = trans ? A->n : A->m, cols = trans ? A->m : A->n;
   KR_CHECK_ARG(x->n == cols && y->n == rows, "krans_spmv: size mismatch");
+  KR_CHECK_ARG(precision == KRANS_PREC_FP64 || precision == KRANS_PREC_MIXED, "krans_spmv: unknown precision");
+  KR_CHECK_ARG(precision != KRANS_PREC_MIXED || A->v32,
+               "krans_spmv: matrix has no FP32 values (create with KRANS_CSR_FP32)");
   krans_ctx *c = A->ctx;
-  const int32_t *rp = trans ? A->rpT : A->rp, *ci = trans ? A->ciT : A->ci;
-  const int lanes = trans ? A->lanesT : A->lanes;
-  const int g = grid_for(c, rows * lanes);
-  if (precision == KRANS_PREC_MIXED) {
-    KR_CHECK_ARG(A->v32, "krans_spmv: matrix has no FP32 values (create with KRANS_CSR_FP32)");
-    spmv_kernel<float, double, double><<<g, 256, 0, c->stream>>>(rows, rp, ci, trans ? A->vT32 : A->v32,
-                                                                 x->d, y->d, lanes, trans ? A->ulenT : A->ulen);
-  } else {
-    spmv_kernel<double, double, double><<<g, 256, 0, c->stream>>>(rows, rp, ci, trans ? A->vT : A->v, x->d,
-                                                                  y->d, lanes, trans ? A->ulenT : A->ulen);
-  }
-  KR_CUDA(cudaGetLastError());
+  KR_CUDA(spmv_launch(spmv_operand(A, trans), precision == KRANS_PREC_MIXED, x->d, y->d, c->sms, c->stream));
+  return KRANS_OK;
+}
+
+int krans_csr_set_spmv_tuning(krans_mat *A, int trans, const krans_spmv_tuning *t) {
+  KR_CHECK_ARG(A && t, "krans_csr_set_spmv_tuning: NULL argument");
+  KR_CHECK_ARG(t->kernel >= KRANS_SPMV_AUTO && t->kernel <= KRANS_SPMV_LANES,
+               "krans_csr_set_spmv_tuning: unknown kernel");
+  KR_CHECK_ARG(t->rows_per_block >= 0 && t->rows_per_block <= 2048,
+               "krans_csr_set_spmv_tuning: rows_per_block outside 0..2048");
+  const int32_t ulen = trans ? A->ulenT : A->ulen;
+  KR_CHECK_ARG(t->kernel != KRANS_SPMV_UNIFORM || ulen == 1 || ulen == 2 || ulen == 4,
+               "krans_csr_set_spmv_tuning: UNIFORM needs every row to hold exactly 1, 2 or 4 entries");
+  (trans ? A->tuneT : A->tune) = *t;
+  return KRANS_OK;
+}
+
+int krans_csr_get_spmv_tuning(const krans_mat *A, int trans, krans_spmv_tuning *t) {
+  KR_CHECK_ARG(A && t, "krans_csr_get_spmv_tuning: NULL argument");
+  *t = trans ? A->tuneT : A->tune;
   return KRANS_OK;
 }
 

@@ -196,15 +196,20 @@ KR_DEV void team_gemm_tn_direct(Team &tm, int64_t n, const double *A, int a, con
 }
 
 
-// S = Z^T Z and G = Z^T (AZ) (p x p, both triangles) in one pass, one warp
-// per 8x8 upper tile with DMMA, operands straight from global memory; each
-// block reduces its fixed row range into a private partial (2 p^2 doubles per
-// block in `part`), summed in block order. Used for short or narrow blocks.
+// S = Z^T Z and G = Z^T (AZ) (p x p) in one pass, one warp per 8x8 tile with
+// DMMA, operands straight from global memory; each block reduces its fixed
+// row range into a private partial (2 p^2 doubles per block in `part`),
+// summed in block order. G is formed on every tile, so its two triangles are
+// computed independently (as Z_i^T (AZ)_j and Z_j^T (AZ)_i) and the tiny
+// GEP's symmetrisation averages them, as the reference's form_gram + 0.5 (G +
+// G^T) does; S is formed on the upper tiles and mirrored (its two triangles
+// would be the same products in the same order). Used for short or narrow
+// blocks.
 template <class Team>
 KR_DEV void team_gram2_direct(Team &tm, int64_t n, const double *Z, const double *AZ, int64_t ld, int p,
                        double *S, double *G, double *part) {
-  const int nt8 = (p + 7) / 8;                       // 8x8 tiles per dimension
-  const int ntiles = nt8 * (nt8 + 1) / 2;            // upper triangle incl. diagonal
+  const int nt8 = (p + 7) / 8; // 8x8 tiles per dimension
+  const int ntiles = nt8 * nt8;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const int ncta = tm.ncta(), rank = tm.cta_rank();
   // fixed row range of this block
@@ -216,13 +221,8 @@ KR_DEV void team_gram2_direct(Team &tm, int64_t n, const double *Z, const double
   // A(row=lane>>2, k=lane&3), B(k=lane&3, col=lane>>2), C rows lane>>2,
   // cols 2*(lane&3) and 2*(lane&3)+1.
   for (int t = wid; t < ntiles; t += nw) {
-    // decode upper-triangular tile index t -> (bi <= bj)
-    int bi = 0, rem = t;
-    while (rem >= nt8 - bi) {
-      rem -= nt8 - bi;
-      bi++;
-    }
-    const int bj = bi + rem;
+    const int bi = t % nt8, bj = t / nt8;
+    const bool upper = bi <= bj; // warp-uniform
     const int ia = bi * 8 + (lane >> 2), jb = bj * 8 + (lane >> 2);
     const bool va = ia < p, vb = jb < p;
     const double *za = Z + (int64_t)(va ? ia : 0) * ld;
@@ -233,40 +233,45 @@ KR_DEV void team_gram2_direct(Team &tm, int64_t n, const double *Z, const double
       const int64_t r = base + (lane & 3);
       const bool in = r < r1;
       const double a = (in && va) ? za[r] : 0.0;
-      const double b = (in && vb) ? zb[r] : 0.0;
       const double ab = (in && vb) ? azb[r] : 0.0;
-      dmma_8x8x4(s0, s1, a, b);
+      if (upper) {
+        const double b = (in && vb) ? zb[r] : 0.0;
+        dmma_8x8x4(s0, s1, a, b);
+      }
       dmma_8x8x4(g0, g1, a, ab);
     }
     const int ci = bi * 8 + (lane >> 2), cj = bj * 8 + 2 * (lane & 3);
     if (ci < p) {
       if (cj < p) {
-        myS[ci + (size_t)cj * p] = s0;
+        if (upper)
+          myS[ci + (size_t)cj * p] = s0;
         myG[ci + (size_t)cj * p] = g0;
       }
       if (cj + 1 < p) {
-        myS[ci + (size_t)(cj + 1) * p] = s1;
+        if (upper)
+          myS[ci + (size_t)(cj + 1) * p] = s1;
         myG[ci + (size_t)(cj + 1) * p] = g1;
       }
     }
   }
   tm.sync();
-  // sum the block partials in block order; fill both triangles
+  // sum the block partials in block order: G entry by entry, S on the upper
+  // triangle (mirrored)
   const int64_t nt = tm.nthreads();
   for (int64_t e = tm.tid(); e < (int64_t)p * p; e += nt) {
     const int j = (int)(e / p), i = (int)(e % p);
-    if (i > j)
-      continue;
     double s = 0.0, g = 0.0;
     for (int b = 0; b < ncta; b++) {
       const double *ps = part + (size_t)b * 2 * p * p;
-      s += __ldcg(ps + e);
       g += __ldcg(ps + (size_t)p * p + e);
+      if (i <= j)
+        s += __ldcg(ps + e);
     }
-    S[i + (size_t)j * p] = s;
-    S[j + (size_t)i * p] = s;
-    G[i + (size_t)j * p] = g;
-    G[j + (size_t)i * p] = g;
+    G[e] = g;
+    if (i <= j) {
+      S[i + (size_t)j * p] = s;
+      S[j + (size_t)i * p] = s;
+    }
   }
   tm.sync();
 }

@@ -74,6 +74,7 @@ struct krans_mat {
   float *v32 = nullptr, *vT32 = nullptr;
   int lanes = 1, lanesT = 1;
   int32_t ulen = 0, ulenT = 0; // uniform row length of A / A^T (0 = not uniform)
+  krans_spmv_tuning tune{}, tuneT{}; // standalone SpMV kernel of A / A^T (zero: automatic)
   char *base = nullptr;         // one device allocation holding every stored array
   size_t bytes = 0;
 };
@@ -92,6 +93,23 @@ struct krans_rng {
 };
 
 namespace kr {
+// One stored operand (A or its transpose) as the standalone SpMV sees it.
+struct SpmvOperand {
+  int64_t rows, cols, nnz;
+  const int32_t *rp, *ci;
+  const double *v64;
+  const float *v32;
+  int lanes;
+  int32_t ulen;
+  krans_spmv_tuning tune;
+};
+inline SpmvOperand spmv_operand(const krans_mat *A, int trans) {
+  return trans ? SpmvOperand{A->n, A->m, A->nnz, A->rpT, A->ciT, A->vT, A->vT32, A->lanesT, A->ulenT, A->tuneT}
+               : SpmvOperand{A->m, A->n, A->nnz, A->rp, A->ci, A->v, A->v32, A->lanes, A->ulen, A->tune};
+}
+// y = op x on `s` (kr_spmv.cu); fp32: FP32 values and sums
+cudaError_t spmv_launch(const SpmvOperand &A, bool fp32, const double *x, double *y, int sms, cudaStream_t s);
+int spmv_rows_per_block(int64_t rows, int64_t nnz);
 // allocation with budget accounting
 int dev_alloc(krans_ctx *ctx, void **p, size_t bytes);
 void dev_free(krans_ctx *ctx, void *p, size_t bytes);

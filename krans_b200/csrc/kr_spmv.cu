@@ -1,0 +1,296 @@
+// Standalone CSR SpMV y = A x / y = A^T x (the stored transpose) behind
+// krans_spmv_ex: MatrixInterface::multiply / multiply_transpose of the
+// reference (include/krans/adapters/eigen/EigenSparseMatrixAdapter.hpp:34-57).
+//
+// The operand arrays (row pointers, columns, values) are read once and are
+// the HBM stream; x is gathered at random and is meant to stay in the 126 MB
+// L2. The streamed loads carry an L2 evict-first policy so they do not push
+// x out of L2, and skip L1.
+//
+// Two kernels, both summing every row in storage order, one product at a
+// time with round-to-nearest multiply and add (no fused multiply-add): the
+// result is bit-identical to the sequential loop `s = 0; s += v[k]*x[c[k]]`
+// compiled without contraction, whatever the launch shape.
+//   uniform  - rows of exactly 1, 2 or 4 entries (incidence and shift
+//              operators): one thread per row, vector loads of the
+//              (column, value) pairs, no row pointers.
+//   row-tile - any rows: a block owns a fixed range of consecutive rows;
+//              it streams their entries in tiles of 2048 with coalesced
+//              loads, stores the products in shared memory, and each thread
+//              then sums the products of its own rows in order (rows longer
+//              than a tile carry their partial sum from tile to tile).
+// A third form, `lanes` threads per row with a warp butterfly, is the one
+// the solver teams use; it is kept selectable for comparison.
+#include <algorithm>
+
+#include "kr_device.cuh"
+#include "kr_internal.h"
+
+namespace kr {
+
+// ---- cache-policy loads of the streamed operand ----------------------------
+KR_DEV uint64_t l2_evict_first_policy() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+KR_DEV int32_t ld_stream(const int32_t *a, uint64_t pol) {
+  int32_t v;
+  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.b32 %0, [%1], %2;" : "=r"(v) : "l"(a), "l"(pol));
+  return v;
+}
+KR_DEV double ld_stream(const double *a, uint64_t pol) {
+  double v;
+  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(a), "l"(pol));
+  return v;
+}
+KR_DEV float ld_stream(const float *a, uint64_t pol) {
+  float v;
+  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(a), "l"(pol));
+  return v;
+}
+KR_DEV int2 ld_stream2(const int32_t *a, uint64_t pol) {
+  int2 v;
+  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.v2.b32 {%0, %1}, [%2], %3;"
+               : "=r"(v.x), "=r"(v.y)
+               : "l"(a), "l"(pol));
+  return v;
+}
+KR_DEV int4 ld_stream4(const int32_t *a, uint64_t pol) {
+  int4 v;
+  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.b32 {%0, %1, %2, %3}, [%4], %5;"
+               : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+               : "l"(a), "l"(pol));
+  return v;
+}
+KR_DEV void ld_stream_pair(const double *a, uint64_t pol, double &x, double &y) {
+  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.v2.f64 {%0, %1}, [%2], %3;"
+               : "=d"(x), "=d"(y)
+               : "l"(a), "l"(pol));
+}
+KR_DEV void ld_stream_pair(const float *a, uint64_t pol, float &x, float &y) {
+  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.v2.f32 {%0, %1}, [%2], %3;"
+               : "=f"(x), "=f"(y)
+               : "l"(a), "l"(pol));
+}
+
+// round-to-nearest product and sum in the accumulation type (never fused)
+KR_DEV double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+KR_DEV float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+KR_DEV double add_rn(double a, double b) { return __dadd_rn(a, b); }
+KR_DEV float add_rn(float a, float b) { return __fadd_rn(a, b); }
+
+constexpr int kSpmvThreads = 256;
+constexpr int kTileNnz = 2048; // entries staged per tile (8 per thread)
+
+// ---- uniform rows ----------------------------------------------------------
+template <int L, class VT>
+__global__ void __launch_bounds__(kSpmvThreads) spmv_uniform_kernel(int64_t rows, const int32_t *__restrict__ ci,
+                                                                    const VT *__restrict__ val,
+                                                                    const double *__restrict__ x,
+                                                                    double *__restrict__ y) {
+  using Acc = VT; // FP64 values: FP64 sums; FP32 values: FP32 sums
+  constexpr int R = 4; // rows in flight per thread
+  const uint64_t pol = l2_evict_first_policy();
+  const int64_t nt = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i0 < rows; i0 += R * nt) {
+    int32_t c[R][L];
+    VT v[R][L];
+#pragma unroll
+    for (int u = 0; u < R; u++) {
+      const int64_t i = i0 + (int64_t)u * nt;
+      if (i < rows) {
+        if constexpr (L == 1) {
+          c[u][0] = ld_stream(ci + i, pol);
+          v[u][0] = ld_stream(val + i, pol);
+        } else if constexpr (L == 2) {
+          const int2 cc = ld_stream2(ci + 2 * i, pol);
+          c[u][0] = cc.x;
+          c[u][1] = cc.y;
+          ld_stream_pair(val + 2 * i, pol, v[u][0], v[u][1]);
+        } else {
+          const int4 cc = ld_stream4(ci + 4 * i, pol);
+          c[u][0] = cc.x;
+          c[u][1] = cc.y;
+          c[u][2] = cc.z;
+          c[u][3] = cc.w;
+          ld_stream_pair(val + 4 * i, pol, v[u][0], v[u][1]);
+          ld_stream_pair(val + 4 * i + 2, pol, v[u][2], v[u][3]);
+        }
+      } else {
+#pragma unroll
+        for (int j = 0; j < L; j++) {
+          c[u][j] = 0;
+          v[u][j] = VT(0);
+        }
+      }
+    }
+    Acc xv[R][L];
+#pragma unroll
+    for (int u = 0; u < R; u++)
+#pragma unroll
+      for (int j = 0; j < L; j++)
+        xv[u][j] = (i0 + (int64_t)u * nt < rows) ? (Acc)__ldg(x + c[u][j]) : Acc(0);
+#pragma unroll
+    for (int u = 0; u < R; u++) {
+      const int64_t i = i0 + (int64_t)u * nt;
+      Acc s = add_rn(Acc(0), mul_rn((Acc)v[u][0], xv[u][0]));
+#pragma unroll
+      for (int j = 1; j < L; j++)
+        s = add_rn(s, mul_rn((Acc)v[u][j], xv[u][j]));
+      if (i < rows)
+        y[i] = (double)s;
+    }
+  }
+}
+
+// ---- row tiles -------------------------------------------------------------
+// Block b owns rows [b*rb, b*rb + rb), rb <= RPT * 256; thread t owns the
+// block's rows t, t + 256, ... (at most RPT of them).
+template <int RPT, class VT>
+__global__ void __launch_bounds__(kSpmvThreads) spmv_rowtile_kernel(int64_t rows, int rb,
+                                                                    const int32_t *__restrict__ rp,
+                                                                    const int32_t *__restrict__ ci,
+                                                                    const VT *__restrict__ val,
+                                                                    const double *__restrict__ x,
+                                                                    double *__restrict__ y) {
+  using Acc = VT;
+  constexpr int NPT = kTileNnz / kSpmvThreads;
+  __shared__ Acc prod[kTileNnz];
+  __shared__ int32_t srp[RPT * kSpmvThreads + 1];
+  const uint64_t pol = l2_evict_first_policy();
+  const int tid = threadIdx.x;
+  for (int64_t blk = blockIdx.x; blk * rb < rows; blk += gridDim.x) {
+    const int64_t r0 = blk * rb;
+    const int nr = (int)imin64(rb, rows - r0);
+    for (int i = tid; i <= nr; i += kSpmvThreads)
+      srp[i] = ld_stream(rp + r0 + i, pol);
+    __syncthreads();
+    const int32_t b = srp[0], e = srp[nr];
+    Acc acc[RPT];
+#pragma unroll
+    for (int u = 0; u < RPT; u++)
+      acc[u] = Acc(0);
+    for (int32_t t0 = b; t0 < e; t0 += kTileNnz) {
+      const int32_t tn = e - t0 < kTileNnz ? e - t0 : kTileNnz;
+      int32_t c[NPT];
+      VT v[NPT];
+#pragma unroll
+      for (int j = 0; j < NPT; j++) {
+        const int q = j * kSpmvThreads + tid;
+        c[j] = q < tn ? ld_stream(ci + t0 + q, pol) : 0;
+        v[j] = q < tn ? ld_stream(val + t0 + q, pol) : VT(0);
+      }
+      Acc xv[NPT];
+#pragma unroll
+      for (int j = 0; j < NPT; j++)
+        xv[j] = (j * kSpmvThreads + tid < tn) ? (Acc)__ldg(x + c[j]) : Acc(0);
+#pragma unroll
+      for (int j = 0; j < NPT; j++) {
+        const int q = j * kSpmvThreads + tid;
+        if (q < tn)
+          prod[q] = mul_rn((Acc)v[j], xv[j]);
+      }
+      __syncthreads();
+#pragma unroll
+      for (int u = 0; u < RPT; u++) {
+        const int lr = tid + u * kSpmvThreads;
+        if (lr < nr) {
+          const int32_t kb = max(srp[lr], t0) - t0, ke = min(srp[lr + 1], t0 + tn) - t0;
+          Acc s = acc[u];
+          for (int32_t k = kb; k < ke; k++)
+            s = add_rn(s, prod[k]);
+          acc[u] = s;
+        }
+      }
+      __syncthreads();
+    }
+#pragma unroll
+    for (int u = 0; u < RPT; u++) {
+      const int lr = tid + u * kSpmvThreads;
+      if (lr < nr)
+        y[r0 + lr] = (double)acc[u];
+    }
+    __syncthreads(); // srp is rewritten by the next row block
+  }
+}
+
+// ---- lanes per row (the solver teams' SpMV) --------------------------------
+struct TeamFlatSpmv {
+  KR_DEV int64_t tid() const { return (int64_t)blockIdx.x * blockDim.x + threadIdx.x; }
+  KR_DEV int64_t nthreads() const { return (int64_t)gridDim.x * blockDim.x; }
+  KR_DEV int64_t warp_id() const { return tid() >> 5; }
+  KR_DEV int64_t nwarps() const { return nthreads() >> 5; }
+};
+template <class VT>
+__global__ void __launch_bounds__(kSpmvThreads) spmv_lanes_kernel(int64_t rows, const int32_t *rp, const int32_t *ci,
+                                                                  const VT *val, const double *x, double *y,
+                                                                  int lanes) {
+  TeamFlatSpmv tm;
+  team_spmv_x(
+      tm, rows, rp, ci, val, [&](int32_t c) { return (VT)x[c]; }, lanes, 0,
+      [&](int64_t i, typename AccOf<VT>::T s) { y[i] = (double)s; });
+}
+
+// Rows per block of the row-tile kernel: about 80% of a tile of entries at
+// the matrix's mean row length, between 32 and 2048 rows.
+int spmv_rows_per_block(int64_t rows, int64_t nnz) {
+  const double mean = rows > 0 ? (double)nnz / (double)rows : 1.0;
+  double rb = 0.8 * kTileNnz / (mean > 0.05 ? mean : 0.05);
+  if (rb < 32)
+    rb = 32;
+  if (rb > 8 * kSpmvThreads)
+    rb = 8 * kSpmvThreads;
+  return (int)rb;
+}
+
+template <class VT>
+static cudaError_t spmv_launch_t(const SpmvOperand &A, const VT *val, const double *x, double *y, int sms,
+                                 cudaStream_t s) {
+  if (A.rows <= 0)
+    return cudaSuccess;
+  int kind = A.tune.kernel;
+  if (kind == KRANS_SPMV_AUTO)
+    kind = (A.ulen == 1 || A.ulen == 2 || A.ulen == 4) ? KRANS_SPMV_UNIFORM : KRANS_SPMV_ROWTILE;
+  if (kind == KRANS_SPMV_UNIFORM && !(A.ulen == 1 || A.ulen == 2 || A.ulen == 4))
+    kind = KRANS_SPMV_ROWTILE;
+  if (kind == KRANS_SPMV_UNIFORM) {
+    // 4 rows in flight per thread; enough blocks for 8 per SM, no more than the rows need
+    const int64_t want = (A.rows + 4 * kSpmvThreads - 1) / (4 * kSpmvThreads);
+    const int g = (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)sms * 8));
+    if (A.ulen == 1)
+      spmv_uniform_kernel<1, VT><<<g, kSpmvThreads, 0, s>>>(A.rows, A.ci, val, x, y);
+    else if (A.ulen == 2)
+      spmv_uniform_kernel<2, VT><<<g, kSpmvThreads, 0, s>>>(A.rows, A.ci, val, x, y);
+    else
+      spmv_uniform_kernel<4, VT><<<g, kSpmvThreads, 0, s>>>(A.rows, A.ci, val, x, y);
+    return cudaGetLastError();
+  }
+  if (kind == KRANS_SPMV_LANES) {
+    const int64_t want = (A.rows * A.lanes + kSpmvThreads - 1) / kSpmvThreads;
+    const int g = (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)sms * 8));
+    spmv_lanes_kernel<VT><<<g, kSpmvThreads, 0, s>>>(A.rows, A.rp, A.ci, val, x, y, A.lanes);
+    return cudaGetLastError();
+  }
+  int rb = A.tune.rows_per_block > 0 ? A.tune.rows_per_block : spmv_rows_per_block(A.rows, A.nnz);
+  rb = std::max(1, std::min(rb, 8 * kSpmvThreads));
+  const int64_t nblk = (A.rows + rb - 1) / rb;
+  const int g = (int)std::min<int64_t>(nblk, 1 << 30);
+  if (rb <= kSpmvThreads)
+    spmv_rowtile_kernel<1, VT><<<g, kSpmvThreads, 0, s>>>(A.rows, rb, A.rp, A.ci, val, x, y);
+  else if (rb <= 2 * kSpmvThreads)
+    spmv_rowtile_kernel<2, VT><<<g, kSpmvThreads, 0, s>>>(A.rows, rb, A.rp, A.ci, val, x, y);
+  else if (rb <= 4 * kSpmvThreads)
+    spmv_rowtile_kernel<4, VT><<<g, kSpmvThreads, 0, s>>>(A.rows, rb, A.rp, A.ci, val, x, y);
+  else
+    spmv_rowtile_kernel<8, VT><<<g, kSpmvThreads, 0, s>>>(A.rows, rb, A.rp, A.ci, val, x, y);
+  return cudaGetLastError();
+}
+
+cudaError_t spmv_launch(const SpmvOperand &A, bool fp32, const double *x, double *y, int sms, cudaStream_t s) {
+  if (fp32)
+    return spmv_launch_t<float>(A, A.v32, x, y, sms, s);
+  return spmv_launch_t<double>(A, A.v64, x, y, sms, s);
+}
+
+} // namespace kr

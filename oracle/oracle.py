@@ -323,3 +323,120 @@ def sym_eig(A):
     Q = np.zeros((n, n), order="F")
     lib().ko_sym_eig(n, A.ctypes.data_as(C.c_void_p), _p(w), Q.ctypes.data_as(C.c_void_p))
     return w, Q
+
+
+# ---------------------------------------------------------------------------
+# The reference's own solver sources compiled against the Eigen-subset shim
+# (oracle/_ref/libkrans_ref.so, built by `make -C oracle ref` from a
+# Deep-SANE/krans checkout; see oracle/ref_driver.cpp). Same options and
+# results as the C restatement above.
+# ---------------------------------------------------------------------------
+REF_LIB = os.path.join(_HERE, "_ref", "libkrans_ref.so")
+_ref_lib = None
+
+
+def build_ref(reference_root):
+    """Compile oracle/_ref from the reference sources under reference_root."""
+    subprocess.run(["make", "-s", "-C", _HERE, "ref", f"REF={reference_root}"], check=True)
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_LIB)
+
+
+def ref_lib():
+    global _ref_lib
+    if _ref_lib is None:
+        if not ref_available():
+            raise OracleError(f"{REF_LIB} is not built (make -C oracle ref REF=<reference root>)")
+        L = C.CDLL(REF_LIB)
+        L.kref_last_error.restype = C.c_char_p
+        L.kref_factory_create.restype = C.c_void_p
+        L.kref_factory_create.argtypes = [C.c_int64, C.c_uint32]
+        L.kref_factory_destroy.argtypes = [C.c_void_p]
+        L.kref_factory_destroy.restype = None
+        L.kref_cyclic.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.kref_lobpcg.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p,
+                                  C.c_void_p, C.c_void_p]
+        _ref_lib = L
+    return _ref_lib
+
+
+class RefFactory:
+    """The reference's StdVectorFactory(default_size, seed): std::mt19937 +
+    std::normal_distribution, state carried across solves."""
+
+    def __init__(self, default_size: int, seed: int):
+        self.h = ref_lib().kref_factory_create(default_size, seed & 0xFFFFFFFF)
+
+    def __del__(self):
+        try:
+            if self.h:
+                ref_lib().kref_factory_destroy(self.h)
+        except Exception:
+            pass
+
+
+def _ref_check(rc):
+    if rc == 1:
+        raise ValueError(ref_lib().kref_last_error().decode())
+    if rc != 0:
+        raise OracleError(ref_lib().kref_last_error().decode())
+
+
+def ref_cyclic(A: Csr, vf: RefFactory, initial_right=None, precond_AAt=None, **kw) -> CyclicResult:
+    """find_nullspace_cyclic_lanczos_ex of the reference itself."""
+    o = KoCyclicOpts()
+    lib().ko_cyclic_opts_default(C.byref(o))
+    for k, v in kw.items():
+        if not hasattr(o, k):
+            raise TypeError(f"unknown cyclic option {k}")
+        setattr(o, k, v)
+    keep = []
+    if initial_right is not None:
+        y0 = np.ascontiguousarray(initial_right, np.float64)
+        keep.append(y0)
+        o.initial_right = _p(y0)
+    cb, pyfn = _wrap_precond(precond_AAt, A.m)
+    o.precond_AAt = cb
+    keep.append(pyfn)
+    k_target = o.nullity_known if o.nullity_known >= 0 else o.k
+    right = np.zeros((max(k_target, 1), A.n), np.float64)
+    left = np.zeros((max(o.k, 1), A.m), np.float64)
+    r = KoCyclicResult()
+    _ref_check(ref_lib().kref_cyclic(C.byref(A.s), C.c_void_p(vf.h), C.byref(o), _p(right), _p(left),
+                                     C.byref(r)))
+    return CyclicResult(right[:r.n_right].copy(), left[:r.n_left].copy(), r.restarts,
+                        r.krylov_steps_total, r.frob_norm_est, bool(r.converged_to_target),
+                        r.cg_solves, r.cg_maxit_hits, r.spmv, r.spmvT)
+
+
+def ref_lobpcg(A: Csr, vf: RefFactory, initial_block=None, M_inv=None, **kw) -> LobpcgResult:
+    """find_nullspace_lobpcg_ex of the reference itself."""
+    o = KoLobpcgOpts()
+    lib().ko_lobpcg_opts_default(C.byref(o))
+    for k, v in kw.items():
+        if not hasattr(o, k):
+            raise TypeError(f"unknown lobpcg option {k}")
+        setattr(o, k, v)
+    keep = []
+    if initial_block is not None:
+        ib = np.ascontiguousarray(np.atleast_2d(initial_block), np.float64)
+        keep.append(ib)
+        o.initial_block = _p(ib)
+        o.n_initial = ib.shape[0]
+    cb, pyfn = _wrap_precond(M_inv, A.n)
+    o.M_inv = cb
+    keep.append(pyfn)
+    cap = max(1, o.nev, o.nullity_known, A.n - o.rank_known if o.rank_known >= 0 else 0)
+    right = np.zeros((cap, A.n), np.float64)
+    theta = np.zeros(cap)
+    resid = np.zeros(cap)
+    r = KoLobpcgResult()
+    _ref_check(ref_lib().kref_lobpcg(C.byref(A.s), C.c_void_p(vf.h), C.byref(o), cap, _p(right), _p(theta),
+                                     _p(resid), C.byref(r)))
+    nr = r.n_right
+    return LobpcgResult(right[:nr].copy(), theta[:nr].copy(), resid[:nr].copy(), r.iters,
+                        r.locked, r.frob_norm_est, r.accept_threshold,
+                        r.best_unaccepted_residual, r.block_size, bool(r.converged_to_target),
+                        r.spmv, r.spmvT)

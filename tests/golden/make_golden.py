@@ -62,4 +62,8 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    ref_root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("KRANS_REFERENCE_ROOT")
+    if not ref_root:
+        sys.exit("usage: make_golden.py REFERENCE_ROOT (or set KRANS_REFERENCE_ROOT): the root of a "
+                 "Deep-SANE/krans checkout, whose data/mat*.ija files are read")
+    main(ref_root)

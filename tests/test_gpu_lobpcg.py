@@ -24,21 +24,27 @@ def solve(ctx, A, vf=None, seed=1, team=0, **kw):
 
 @pytest.mark.parametrize("team", TEAMS)
 def test_quickstart_cyclic_then_lobpcg_same_factory(ctx, oracle, team):
+    # examples/quickstart.cpp: cyclic, then LOBPCG on the same factory (the
+    # LOBPCG start block comes from the RNG state cyclic left behind); both at
+    # the accuracy bound tol_abs = 1e-12 L, tol_rel = 0
     import krans_b200 as kb
     inst = G.shift_operator(1000, 3, 0.5)
+    A2 = inst.A.multiply(inst.A)
+    L = float(np.sqrt(max(A2.sum(axis=0).max(), A2.sum(axis=1).max())))
     M = kb.CudaCsrMatrixAdapter.from_scipy(ctx, inst.A)
     vf = kb.CudaVectorFactory(ctx, 1000, seed=42)
-    kb.find_nullspace_cyclic_lanczos(M, vf, kb.CyclicLanczosOptions(k=3, team=team))
-    R = kb.find_nullspace_lobpcg_ex(M, vf, kb.LOBPCGOptions(nev=3, team=team))
+    kb.find_nullspace_cyclic_lanczos(M, vf, kb.CyclicLanczosOptions(k=3, team=team, tol_abs=1e-12 * L, tol_rel=0.0))
+    R = kb.find_nullspace_lobpcg_ex(M, vf, kb.LOBPCGOptions(nev=3, team=team, tol_abs=1e-12 * L, tol_rel=0.0))
     U = kb.basis_to_numpy(R.right_null)
     assert U.shape[0] == 3 and R.converged_to_target
-    assert max(np.linalg.norm(inst.A @ u) for u in U) < 1e-9  # README: 3.5e-11
-    assert oracle.subspace_dist(inst.kernel, U) < 1e-9          # README: 6.4e-11
+    assert max(np.linalg.norm(inst.A @ u) for u in U) <= 1e-12 * L
+    assert oracle.subspace_dist(inst.kernel, U) <= 1e-10
     Ao = oracle.Csr.from_scipy(inst.A)
     rng = oracle.Rng(42)
-    oracle.cyclic(Ao, rng, k=3)
-    O = oracle.lobpcg(Ao, rng, nev=3)
-    assert oracle.subspace_dist(O.right_null, U) < 1e-9
+    oracle.cyclic(Ao, rng, k=3, tol_abs=1e-12 * L, tol_rel=0.0)
+    O = oracle.lobpcg(Ao, rng, nev=3, tol_abs=1e-12 * L, tol_rel=0.0)
+    assert oracle.subspace_dist(O.right_null, U) <= 1e-10
+    assert oracle.subspace_diff_rref(O.right_null, U) <= 1e-8
     assert R.block_size == O.block_size == 3
 
 
