@@ -137,91 +137,149 @@ DRAM_PER_ALGO_BYTE = 1.607e12 / 3.966e12
 
 
 # ---------------------------------------------------------------------------
-def cpu_baseline_sample(insts, seconds, precision_label="fp64"):
-    """The CPU oracle (a plain-C restatement of the reference's cyclic solver,
-    single-threaded) on a bounded sample of the workload."""
-    from oracle import oracle as O
-    O.build()
-    t0 = time.perf_counter()
-    done = 0
-    for i, inst in enumerate(insts):
-        A = O.Csr.from_scipy(inst.A)
-        L = lower_norm_bound(inst.A)
-        O.cyclic(A, O.Rng(1000 + i), k=inst.k, tol_abs=1e-12 * L, tol_rel=0.0, cg_maxit=1000)
-        done += 1
-        if time.perf_counter() - t0 > seconds:
-            break
-    dt = time.perf_counter() - t0
-    return done, dt
+def reference_sample(batches, warmup, steps, seed):
+    """The instances the CPU arms solve: one per timed step, stratified over
+    the whole size range of that step's batch. The batch's instances are
+    ranked by nnz and cut into S = min(8, steps) equal strata; timed step t
+    takes stratum t mod S and one instance drawn from it (seeded). Both arms
+    use this list: the reference arm times these instances, and the GPU arm
+    also reports its rate on exactly them. Returns [(step, index, stratum)]."""
+    S = max(1, min(8, steps))
+    out = []
+    for t in range(steps):
+        insts = batches[warmup + t]
+        order = sorted(range(len(insts)), key=lambda i: (insts[i].A.nnz, i))
+        j = t % S
+        lo, hi = (j * len(order)) // S, ((j + 1) * len(order)) // S
+        r = np.random.Generator(np.random.PCG64([seed, 4099, t]))
+        out.append((warmup + t, order[int(r.integers(lo, max(lo + 1, hi)))], j))
+    return out, S
 
 
-def _oracle_worker(args):
-    A_parts, k, seed = args
+def stratified_rate(times, strata, S, cores):
+    """Solves/s of `cores` independent single-threaded workers on the batches
+    the sample was drawn from: cores / E[t], with E[t] the mean over strata of
+    each stratum's mean time (every stratum holds 1/S of the instances)."""
+    per = {}
+    for t, j in zip(times, strata):
+        per.setdefault(j, []).append(t)
+    means = [float(np.mean(v)) for v in per.values()]
+    et = float(np.mean(means)) if means else float("inf")
+    return cores / et, {str(j): float(np.mean(v)) for j, v in sorted(per.items())}
+
+
+def _ref_available():
+    try:
+        from oracle import oracle as O
+        return O.ref_available()
+    except Exception:
+        return False
+
+
+def _cpu_worker(args):
+    """One instance on one host thread: the reference's own solver sources
+    (oracle/_ref) when built, else the C restatement. Returns (seconds,
+    converged)."""
+    A_parts, k, seed, kind = args
     import scipy.sparse as sp
     sys.path.insert(0, ROOT)
     from oracle import oracle as O
     m, n, indptr, indices, data = A_parts
     A = sp.csr_matrix((data, indices, indptr), shape=(m, n))
     L = lower_norm_bound(A)
+    Ao = O.Csr.from_scipy(A)
+    kw = dict(k=k, tol_abs=1e-12 * L, tol_rel=0.0, cg_maxit=1000)
     t = time.perf_counter()
-    R = O.cyclic(O.Csr.from_scipy(A), O.Rng(seed), k=k, tol_abs=1e-12 * L, tol_rel=0.0, cg_maxit=1000)
+    if kind == "reference":
+        R = O.ref_cyclic(Ao, O.RefFactory(n, seed), **kw)
+    else:
+        R = O.cyclic(Ao, O.Rng(seed), **kw)
     return time.perf_counter() - t, int(R.right_null.shape[0] == k)
 
 
+def _job(inst, seed, kind):
+    A = inst.A
+    return ((A.shape[0], A.shape[1], A.indptr, A.indices, A.data), inst.k, seed, kind)
+
+
+def cpu_baseline_sample(insts, seconds):
+    """Single host thread on a bounded sample (smallest first until `seconds`
+    of CPU work): the reported cpu_baseline of the GPU arm."""
+    kind = "reference" if _ref_available() else "port"
+    t0 = time.perf_counter()
+    done = 0
+    for i, inst in enumerate(sorted(insts, key=lambda x: x.A.nnz)):
+        _cpu_worker(_job(inst, 1000 + i, kind))
+        done += 1
+        if time.perf_counter() - t0 > seconds:
+            break
+    return done, time.perf_counter() - t0, kind
+
+
 def run_reference(args):
-    """--impl reference: the reference algorithm on the CPU (the C oracle; the
-    reference itself needs Eigen, absent here), all host cores, bounded
-    sample per step."""
+    """--impl reference: the reference's cyclic solver on the host CPU, all
+    cores (one single-threaded instance per core), on the instances of
+    reference_sample() drawn from the same batches the GPU arm solves. The
+    reference's own sources compiled against the Eigen-subset shim
+    (oracle/_ref) when built, else the C restatement. Every sampled instance
+    goes to one pool at once, largest stratum first, and the rate comes from
+    the per-instance times (stratified_rate), so idle cores at the end of the
+    run do not count against it."""
     import multiprocessing as mp
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
     from oracle import oracle as O
     O.build()
+    kind = "reference" if O.ref_available() else "port"
     cores = os.cpu_count() or 1
     batches = make_batches(args.warmup + args.steps, args.batch, args.seed)
+    sample, S = reference_sample(batches, args.warmup, args.steps, args.seed)
     ctx = mp.get_context("spawn")
-    per_step = []
-    solved = 0
     with ctx.Pool(cores) as pool:
-        for s, insts in enumerate(batches):
-            # bounded sample: stratified by nnz over the smaller 75% of the
-            # batch (the largest quarter takes minutes per instance on one
-            # core); warm-up steps run the smallest instance only (the CPU
-            # path has nothing to warm beyond the page cache)
-            order = sorted(range(len(insts)), key=lambda i: insts[i].A.nnz)
-            order = order[: max(1, (3 * len(order)) // 4)]
-            stride = max(1, len(order) // max(1, args.ref_sample))
-            pick = [order[i] for i in range(stride // 2, len(order), stride)][: args.ref_sample]
-            if s < args.warmup:
-                pick = order[:1]
-            jobs = [((insts[i].A.shape[0], insts[i].A.shape[1], insts[i].A.indptr, insts[i].A.indices,
-                      insts[i].A.data), insts[i].k, 1000 + i) for i in pick]
-            t = time.perf_counter()
-            res = pool.map(_oracle_worker, jobs, chunksize=1)
-            dt = time.perf_counter() - t
-            if s >= args.warmup:
-                per_step.append((len(jobs), dt))
-                solved += sum(r[1] for r in res)
-    n = sum(p[0] for p in per_step)
-    T = sum(p[1] for p in per_step)
-    v = n / T if T > 0 else 0.0
+        # warm-up: the smallest instance of each warm-up batch (page cache, imports)
+        warm = [_job(min(batches[w], key=lambda x: x.A.nnz), 7, kind) for w in range(args.warmup)]
+        pool.map(_cpu_worker, warm, chunksize=1)
+        order = sorted(range(len(sample)), key=lambda q: -sample[q][2])
+        jobs = [_job(batches[st][ix], 1000 + ix, kind) for (st, ix, _) in (sample[q] for q in order)]
+        t0 = time.perf_counter()
+        res = pool.map(_cpu_worker, jobs, chunksize=1)
+        wall = time.perf_counter() - t0
+    times = [r[0] for r in res]
+    strata = [sample[q][2] for q in order]
+    v, per_stratum = stratified_rate(times, strata, S, cores)
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": "solves/s",
         "higher_is_better": True, "n_gpus": 0, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1e3 * T / max(1, len(per_step)), "dtype": "f64", "data": "synthetic",
-        "config": dict(batched_config(args, 1), sample_per_step=args.ref_sample),
-        "cpu_baseline": {"value": v, "unit": "solves/s", "cores": cores, "kind": "port",
-                         "sample": f"{args.ref_sample} instances per step, stratified by nnz over the smaller "
-                                   f"75% of each {args.batch}-instance batch, one process per core"},
+        "ms_per_step": 1e3 * wall / max(1, args.steps), "dtype": "f64", "data": "synthetic",
+        "config": batched_config(args, 1),
+        "cpu_baseline": {"value": v, "unit": "solves/s", "cores": cores, "kind": kind,
+                         "sample": f"{len(sample)} instances, one per timed step, stratified over the whole nnz "
+                                   f"range of that step's {args.batch}-instance batch ({S} strata); rate = cores / "
+                                   f"mean over strata of the per-instance single-thread time",
+                         "per_stratum_mean_s": per_stratum, "wall_s": wall, "cpu_s": float(sum(times))},
         "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "converged": solved, "vs_baseline": None,
+        "converged": int(sum(r[1] for r in res)), "sampled": len(res), "vs_baseline": None,
     }
     print(json.dumps(line), flush=True)
     return 0
 
 
 # ---------------------------------------------------------------------------
+def reduce_over_ranks(dist, maxes, sums, device):
+    """Max over ranks of `maxes` (device times) and sum of `sums` (counts);
+    with no process group, the local values."""
+    if dist is None:
+        return list(maxes), list(sums)
+    import torch
+    dev = device if dist.get_backend() == "nccl" else "cpu"
+    a = torch.tensor(list(maxes), dtype=torch.float64, device=dev)
+    b = torch.tensor(list(sums), dtype=torch.float64, device=dev)
+    dist.all_reduce(a, op=dist.ReduceOp.MAX)
+    dist.all_reduce(b, op=dist.ReduceOp.SUM)
+    return a.tolist(), b.tolist()
+
+
 def batched_config(args, world):
     return {"workload": WORKLOAD, "batch_per_step": args.batch, "form": "mixed-precision batched",
             "accept": "tol_abs=1e-12*max(row,col norm), tol_rel=0, cg_maxit=1000",
@@ -286,33 +344,41 @@ def run_ours(args):
     barrier()
     clocks = clk.summary()
     T = sum(dev_ms) / 1e3
-    if dist is not None:
-        import torch
-        t = torch.tensor([T, float(nsolves), float(ok)], dtype=torch.float64, device=f"cuda:{local}")
-        tmax = t.clone()
-        dist.all_reduce(tmax[:1], op=dist.ReduceOp.MAX)
-        dist.all_reduce(t[1:], op=dist.ReduceOp.SUM)
-        T, nsolves_all, ok_all = float(tmax[0]), int(t[1]), int(t[2])
-    else:
-        nsolves_all, ok_all = nsolves, ok
+    (T,), (nsolves_all, ok_all) = reduce_over_ranks(dist, [T], [nsolves, ok], f"cuda:{local}")
+    nsolves_all, ok_all = int(nsolves_all), int(ok_all)
     value = nsolves_all / T if T > 0 else 0.0
 
-    # ---- plain FP64 GPU path, one request at a time, stratified sample
-    first = batches[args.warmup]
-    order = sorted(range(len(first)), key=lambda i: first[i].A.nnz)
-    stride = max(1, len(order) // max(1, args.plain_sample))
-    pick = [order[i] for i in range(stride // 2, len(order), stride)][: args.plain_sample]
+    # ---- the CPU arms' sample (one instance per timed step, stratified over
+    # each batch's size range): the plain FP64 path one request at a time,
+    # and the batched mixed form on exactly these instances
+    sample, _ = reference_sample(batches, args.warmup, args.steps, args.seed)
     plain_ms = []
-    for i in pick:
-        inst = first[i]
-        M = reqs[args.warmup][i].A
+    for (st, i, _) in sample:
+        inst = batches[st][i]
         vf = kb.CudaVectorFactory(ctx, inst.A.shape[1], seed=1 + i, mode="philox")
-        R = kb.find_nullspace_cyclic_lanczos_ex(M, vf, opts_for(inst, 0))
+        R = kb.find_nullspace_cyclic_lanczos_ex(reqs[st][i].A, vf, opts_for(inst, 0))
         plain_ms.append(R.device_ms)
     plain_value = len(plain_ms) / (sum(plain_ms) / 1e3) if plain_ms else None
-    # same sample on the batched mixed form, for a like-for-like ratio
-    sample_reqs = build_reqs([first[i] for i in pick], 1, 99)
+    sample_insts = [batches[st][i] for (st, i, _) in sample]
+    sample_reqs = build_reqs(sample_insts, 1, 99)
     ms_sample = solve_batch(ctx, sample_reqs)
+    sample_ok = sum(int(r.result.converged_to_target and r.result.n_right == inst.k)
+                    for r, inst in zip(sample_reqs, sample_insts))
+    del sample_reqs
+
+    # ---- what precision buys beside batching: the first timed batch again in
+    # FP64 (same launches, same seeds), and each mixed result's distance to the
+    # FP64 result of the same request
+    first = batches[args.warmup]
+    fp64_reqs = [SolveRequest(rq.A, opts_for(inst, 0), seed=rq.seed, rng_mode="philox")
+                 for inst, rq in zip(first, reqs[args.warmup])]
+    ms_fp64 = solve_batch(ctx, fp64_reqs)
+    dists = []
+    for inst, rm, rf in zip(first, reqs[args.warmup], fp64_reqs):
+        if rm.result.n_right == inst.k and rf.result.n_right == inst.k and inst.k > 0:
+            Um, Uf = rm.basis(), rf.basis()
+            dists.append(float(np.linalg.norm(Um - (Um @ Uf.T) @ Uf, 2)))
+    del fp64_reqs
 
     # ---- end to end through the public API with host buffers (pinned)
     try:
@@ -382,18 +448,32 @@ def run_ours(args):
                        "definition": "launch start -> request done, device clock"},
         "accuracy": {"converged": ok_all, "solves": nsolves_all, "max_rel_residual": worst},
         "plain_fp64": {"value": plain_value, "unit": "solves/s", "sample": len(plain_ms),
-                       "p50_ms": percentile(plain_ms, 50), "p99_ms": percentile(plain_ms, 99),
-                       "speedup_batched_mixed_same_sample": (len(pick) / (ms_sample / 1e3)) / plain_value
-                       if plain_value and ms_sample > 0 else None},
+                       "definition": "FP64, one request at a time (find_nullspace_cyclic_lanczos_ex), on the "
+                                     "CPU arms' stratified sample",
+                       "p50_ms": percentile(plain_ms, 50), "p99_ms": percentile(plain_ms, 99)},
+        "on_reference_sample": {"value": len(sample) / (ms_sample / 1e3) if ms_sample > 0 else None,
+                                "unit": "solves/s", "instances": len(sample), "converged": sample_ok,
+                                "definition": "mixed-precision batched launch over exactly the instances the "
+                                              "reference arm times"},
+        "batched_fp64": {"value": len(first) / (ms_fp64 / 1e3) if ms_fp64 > 0 else None, "unit": "solves/s",
+                         "instances": len(first),
+                         "definition": "the first timed batch in one FP64 batched launch (mixed form on the same "
+                                       "batch: value of that step)"},
+        "mixed_vs_fp64_subspace_dist": {"max": max(dists) if dists else None,
+                                        "p99": percentile(dists, 99), "compared": len(dists),
+                                        "within_1e-10": int(sum(d <= 1e-10 for d in dists)),
+                                        "definition": "largest principal-angle sine between each mixed-precision "
+                                                      "basis and the FP64 basis of the same request"},
         "speedup_vs_plain_fp64": value / plain_value if plain_value else None,
         "e2e": e2e, "roofline": roofline, "clocks": clocks,
         "gpu_launches": 2 * args.steps,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        done, dt = cpu_baseline_sample([first[i] for i in pick], args.cpu_seconds)
-        line["cpu_baseline"] = {"value": done / dt, "unit": "solves/s", "cores": 1, "kind": "port",
-                                "sample": f"{done} of {len(pick)} stratified instances of the first timed batch "
-                                          f"(C oracle, single thread)"}
+        done, dt, kind = cpu_baseline_sample(sample_insts, args.cpu_seconds)
+        line["cpu_baseline"] = {"value": done / dt, "unit": "solves/s", "cores": 1, "kind": kind,
+                                "sample": f"{done} of the {len(sample_insts)} sampled instances, smallest first, "
+                                          f"{args.cpu_seconds:.0f} s budget, single thread (smaller than average: "
+                                          f"flatters the CPU)"}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist is not None:
@@ -815,6 +895,20 @@ def run_serving(args):
 
 
 # ---------------------------------------------------------------------------
+def launch_ranks(n):
+    """`bench.py --gpus N` started without a launcher: re-run this command as
+    N ranks, one per GPU, through torch.distributed.run on 127.0.0.1 (the
+    same environment contract as an external torchrun launch). Rank 0 prints
+    the JSON line."""
+    import socket
+    with socket.socket() as so:
+        so.bind(("127.0.0.1", 0))
+        port = so.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={n}",
+           "--master-addr=127.0.0.1", f"--master-port={port}", os.path.abspath(__file__), *sys.argv[1:]]
+    return subprocess.call(cmd)
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -823,8 +917,6 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--batch", type=int, default=256)
     ap.add_argument("--seed", type=int, default=1)
-    ap.add_argument("--plain-sample", type=int, default=16)
-    ap.add_argument("--ref-sample", type=int, default=16)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", choices=["batched", "quickstart", "lobpcg", "planted", "serving", "spmv"],
@@ -844,6 +936,8 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        return launch_ranks(args.gpus)
     if args.impl == "reference":
         return run_reference(args)
     if args.workload != "batched":

@@ -1,6 +1,8 @@
-"""bench.py's reference arm runs the CPU oracle only, so its JSON contract is
+"""bench.py's reference arm runs on the CPU only, so its JSON contract is
 checked here on a tiny sample: same metric, unit and config as the GPU arm,
-plus the keys of the reference arm."""
+plus the keys of the reference arm. The replica path of the GPU arm (per-rank
+seeds, max of device times and sum of counts over ranks) is checked with two
+gloo ranks."""
 import json
 import os
 import subprocess
@@ -12,18 +14,37 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 def test_reference_arm_json_line():
     sys.path.insert(0, ROOT)
     import bench
+    # seed 3, batch 4: the one sampled instance is the smallest (nnz 2270)
     out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "1",
-                          "--warmup", "0", "--batch", "8", "--ref-sample", "1"],
+                          "--warmup", "0", "--batch", "4", "--seed", "3"],
                          capture_output=True, text=True, timeout=900, cwd=ROOT)
     assert out.returncode == 0, out.stderr[-2000:]
     line = json.loads([l for l in out.stdout.splitlines() if l.startswith("{")][-1])
     assert line["impl"] == "reference"
     assert line["metric"] == bench.METRIC and line["unit"] == "solves/s" and line["higher_is_better"] is True
     assert line["value"] > 0 and line["cpu_baseline"]["value"] == line["value"]
-    assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["cores"] >= 1
+    assert line["cpu_baseline"]["kind"] == ("reference" if bench._ref_available() else "port")
+    assert line["cpu_baseline"]["cores"] >= 1 and line["sampled"] == 1 and line["converged"] == 1
     assert line["e2e"] == {"value": line["value"], "unit": "solves/s", "h2d_bytes_per_step": 0,
                            "d2h_bytes_per_step": 0}
-    assert line["config"]["workload"] == bench.WORKLOAD
+
+    class A:
+        batch = 4
+    assert line["config"] == bench.batched_config(A, 1)  # identical to the GPU arm's config
+
+
+def test_reference_sample_and_rate():
+    sys.path.insert(0, ROOT)
+    import bench
+    batches = bench.make_batches(3 + 5, 16, 9)
+    s1, S = bench.reference_sample(batches, 3, 5, 9)
+    s2, _ = bench.reference_sample(batches, 3, 5, 9)
+    assert s1 == s2 and S == 5 and [x[0] for x in s1] == [3, 4, 5, 6, 7]
+    for (st, i, j) in s1:  # the instance lies in its stratum of the step's batch
+        order = sorted(range(16), key=lambda q: (batches[st][q].A.nnz, q))
+        assert (j * 16) // S <= order.index(i) < ((j + 1) * 16) // S
+    v, per = bench.stratified_rate([1.0, 3.0, 2.0, 4.0], [0, 0, 1, 1], 2, 8)
+    assert per == {"0": 2.0, "1": 3.0} and abs(v - 8 / 2.5) < 1e-12
 
 
 def test_indicator_kernel_distance():
