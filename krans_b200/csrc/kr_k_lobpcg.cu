@@ -7,10 +7,18 @@
 
 namespace kr {
 
+// dynamic shared memory of the LOBPCG kernels: the tiles of the Gram and Z * Y products
+static cudaError_t lobpcg_grid_smem_attr() {
+  static cudaError_t e = cudaFuncSetAttribute((const void *)lobpcg_grid_kernel,
+                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lobpcg_dyn_smem_bytes());
+  return e;
+}
+
 int lobpcg_grid_blocks(krans_ctx *ctx, int threads) {
   int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)lobpcg_grid_kernel, threads, 0) !=
-          cudaSuccess ||
+  if (lobpcg_grid_smem_attr() != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)lobpcg_grid_kernel, threads,
+                                                    lobpcg_dyn_smem_bytes()) != cudaSuccess ||
       per_sm < 1) {
     cudaGetLastError();
     per_sm = 1;
@@ -23,8 +31,12 @@ cudaError_t launch_lobpcg_cta(const LobpcgDesc *d_dev, int threads, cudaStream_t
 cudaError_t launch_lobpcg(bool grid, const LobpcgDesc &d, const LobpcgDesc *d_dev, int blocks, int threads,
                           cudaStream_t s) {
   if (grid) {
+    cudaError_t e = lobpcg_grid_smem_attr();
+    if (e != cudaSuccess)
+      return e;
     void *args[] = {(void *)&d};
-    return cudaLaunchCooperativeKernel((const void *)lobpcg_grid_kernel, dim3(blocks), dim3(threads), args, 0, s);
+    return cudaLaunchCooperativeKernel((const void *)lobpcg_grid_kernel, dim3(blocks), dim3(threads), args,
+                                       lobpcg_dyn_smem_bytes(), s);
   }
   return launch_lobpcg_cta(d_dev, threads, s);
 }

@@ -6,7 +6,11 @@
 namespace kr {
 
 cudaError_t launch_lobpcg_cta(const LobpcgDesc *d_dev, int threads, cudaStream_t s) {
-  lobpcg_cta_kernel<<<1, threads, 0, s>>>(d_dev);
+  static const cudaError_t attr = cudaFuncSetAttribute(
+      (const void *)lobpcg_cta_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lobpcg_dyn_smem_bytes());
+  if (attr != cudaSuccess)
+    return attr;
+  lobpcg_cta_kernel<<<1, threads, lobpcg_dyn_smem_bytes(), s>>>(d_dev);
   return cudaGetLastError();
 }
 

@@ -72,6 +72,12 @@ template <class Team> struct LobpcgSolver {
     c.bytes += 16.0 * n;
     tm.sync();
   }
+  // k consecutive columns (ld ldn) in one pass; src and dst must not overlap
+  KR_DEV void copy_cols(const double *s, double *dd, int64_t k) {
+    team_for(tm, k * ldn, [&](int64_t i) { dd[i] = s[i]; });
+    c.bytes += 16.0 * n * k;
+    tm.sync();
+  }
   KR_DEV void scale(double a, double *x) {
     team_for(tm, n, [&](int64_t i) { x[i] *= a; });
     c.bytes += 16.0 * n;
@@ -335,7 +341,10 @@ template <class Team> struct LobpcgSolver {
 
   // one Cholesky-QR round: out = V chol(V^T V)^-T (V unchanged)
   __device__ __noinline__ bool cholqr_round(const double *V, int64_t k, double tol, double *out) {
-    team_gemm_tn(tm, n, V, (int)k, V, (int)k, ldn, d.Sj, d.gram_part);
+    if (n >= 131072 && k >= 32)
+      team_gram_sym_tiled(tm, n, V, nullptr, ldn, (int)k, d.Sj, nullptr, d.gram_part);
+    else
+      team_gemm_tn(tm, n, V, (int)k, V, (int)k, ldn, d.Sj, d.gram_part);
     gram_flops += 2.0 * (double)n * k * k;
     c.bytes += 8.0 * n * k;
     if (!chol_inv_t((int)k, tol))
@@ -377,8 +386,7 @@ template <class Team> struct LobpcgSolver {
   __device__ __noinline__ void form_gram(const double *Zb, const double *AZb, int p) {
     const uint64_t t0 = globaltimer_ns();
     if (n >= 131072 && p >= 32) {
-      team_gemm_tn(tm, n, Zb, p, Zb, p, ldn, d.S, d.gram_part);
-      team_gemm_tn(tm, n, Zb, p, AZb, p, ldn, d.G, d.gram_part);
+      team_gram_sym_tiled(tm, n, Zb, AZb, ldn, p, d.S, d.G, d.gram_part); // both in one pass
     } else {
       team_gram2_direct(tm, n, Zb, AZb, ldn, p, d.S, d.G, d.gram_part); // both in one pass
     }
@@ -517,6 +525,21 @@ template <class Team> struct LobpcgSolver {
     team_combine(tm, n, Zb, ldn, zc, Y, ldy, roff, q, out);
     c.bytes += (double)(zc + q) * 8.0 * n;
     tm.sync();
+  }
+
+  // X <- X Y and AX <- AX Y with Y the tiny GEP's eigenvectors (d.Ym, ld
+  // bs): the reference recomputes AX = N (X Y) with bs operator pairs
+  // (LOBPCGSolver.cpp:520-521, 779-781); N (X Y) = (N X) Y, so one more
+  // product gives it. The three blocks trade places instead of being copied.
+  __device__ __noinline__ void rotate_block(double *&X, double *&AX, double *&T, int bs) {
+    combine(X, bs, d.Ym, bs, 0, bs, T);
+    double *t = X;
+    X = T;
+    T = t;
+    combine(AX, bs, d.Ym, bs, 0, bs, T);
+    t = AX;
+    AX = T;
+    T = t;
   }
 
   KR_DEV void theta_from(int64_t bs, int tn) {
@@ -747,10 +770,7 @@ template <class Team> struct LobpcgSolver {
       err = kLobErrGep;
       goto finish;
     }
-    combine(X, (int)bs, d.Ym, (int)bs, 0, (int)bs, T1);
-    for (int64_t j = 0; j < bs; j++)
-      copy(col(T1, j), col(X, j));
-    apply_normal(X, bs, AX);
+    rotate_block(X, AX, T1, (int)bs);
     theta_from(bs, (int)bs);
 
     while (nlocked < k_target && its < o.max_iters && tm.ok()) {
@@ -847,23 +867,19 @@ template <class Team> struct LobpcgSolver {
       for (int64_t j = ini; j < bs; j++)
         apply_minv(col(Rb, j), col(W, j));
       const int64_t na = bs - ini;
-      for (int64_t t = 0; t < na; t++)
-        copy(col(W, ini + t), col(T1, t));
+      copy_cols(col(W, ini), T1, na);
       if (!orthonormalize_block(T1, na, d.Yl, nlocked, o.gs_tol, o.gs_reorth != 0, T2)) {
         for (int64_t j = ini; j < bs; j++)
           random(col(W, j));
         for (int64_t j = ini; j < bs; j++)
           gs_pass(d.Yl, nlocked, col(W, j));
       } else {
-        for (int64_t t = 0; t < na; t++)
-          copy(col(T1, t), col(W, ini + t));
+        copy_cols(T1, col(W, ini), na);
       }
       if (its > 1) {
-        for (int64_t t = 0; t < na; t++)
-          copy(col(P, ini + t), col(T1, t));
+        copy_cols(col(P, ini), T1, na);
         (void)orthonormalize_block(T1, na, d.Yl, nlocked, o.gs_tol, o.gs_reorth != 0, T2);
-        for (int64_t t = 0; t < na; t++)
-          copy(col(T1, t), col(P, ini + t));
+        copy_cols(T1, col(P, ini), na);
       }
       const int64_t np = (its > 1) ? na : 0;
       const int64_t nv = na + na + np;
@@ -874,12 +890,10 @@ template <class Team> struct LobpcgSolver {
         goto finish;
       }
       // Z = [X_act | W_act | P_act] (contiguous copy)
-      for (int64_t t = 0; t < na; t++) {
-        copy(col(X, ini + t), col(d.Z, t));
-        copy(col(W, ini + t), col(d.Z, na + t));
-        if (np)
-          copy(col(P, ini + t), col(d.Z, 2 * na + t));
-      }
+      copy_cols(col(X, ini), d.Z, na);
+      copy_cols(col(W, ini), col(d.Z, na), na);
+      if (np)
+        copy_cols(col(P, ini), col(d.Z, 2 * na), na);
       apply_normal(d.Z, nv, d.AZ);
       form_gram(d.Z, d.AZ, (int)nv);
       if (!tiny_gep((int)nv)) {
@@ -891,13 +905,12 @@ template <class Team> struct LobpcgSolver {
         // P_new = [W P] [Yw; Yp]; X_new = X_act Yx + P_new
         combine(d.Z + na * ldn, (int)(na + np), d.Ym, (int)nv, (int)na, (int)take, T1);
         combine(d.Z, (int)na, d.Ym, (int)nv, 0, (int)take, T2);
-        for (int64_t j = 0; j < take; j++)
-          copy(col(T1, j), col(P, ini + j));
-        for (int64_t j = 0; j < take; j++) {
-          double *xo = col(X, ini + j);
-          const double *a = col(T2, j), *b = col(P, ini + j);
-          team_for(tm, n, [&](int64_t i) { xo[i] = a[i] + b[i]; });
-          c.bytes += 24.0 * n;
+        copy_cols(T1, col(P, ini), take);
+        {
+          double *xo = col(X, ini);
+          const double *a = T2, *b = col(P, ini);
+          team_for(tm, take * ldn, [&](int64_t i) { xo[i] = a[i] + b[i]; });
+          c.bytes += 24.0 * n * take;
           tm.sync();
         }
         if (!orthonormalize_block(X + ini * ldn, take, d.Yl, nlocked, o.gs_tol, o.gs_reorth != 0, T1)) {
@@ -912,10 +925,7 @@ template <class Team> struct LobpcgSolver {
         err = kLobErrGep;
         goto finish;
       }
-      combine(X, (int)bs, d.Ym, (int)bs, 0, (int)bs, T1);
-      for (int64_t j = 0; j < bs; j++)
-        copy(col(T1, j), col(X, j));
-      apply_normal(X, bs, AX);
+      rotate_block(X, AX, T1, (int)bs);
       theta_from(bs, (int)bs);
     }
     R.converged = (R.locked >= k_target) ? 1 : 0;

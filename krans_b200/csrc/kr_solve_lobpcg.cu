@@ -56,9 +56,10 @@ static size_t lobpcg_layout(int64_t m, int64_t n, int64_t bs, int64_t k, int64_t
   t.eig_pq = c.take<int32_t>(2 * (pmax / 2 + 2));
   t.eig_ord = c.take<int32_t>(pmax + 4);
   {
-    // partials of the tiled A^T B: up to (2 ncta + tiles) tiles of 64 x 64
+    // partials of the tiled products: up to (2 ncta + tiles) items of one
+    // 64 x 64 tile (A^T B) or two (S and G of the Gram)
     const int64_t tiles = ((pmax + 63) / 64) * ((pmax + 63) / 64);
-    t.gram_part = c.take<double>(std::max<int64_t>((int64_t)ncta * 2 * pmax * pmax, (2 * (int64_t)ncta + tiles) * 4096));
+    t.gram_part = c.take<double>(std::max<int64_t>((int64_t)ncta * 2 * pmax * pmax, (2 * (int64_t)ncta + tiles) * 8192));
   }
   t.theta_out = c.take<double>(std::max<int64_t>(k, 1));
   t.resid_out = c.take<double>(std::max<int64_t>(k, 1));
