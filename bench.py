@@ -466,6 +466,7 @@ def run_ours(args):
                                                       "basis and the FP64 basis of the same request"},
         "speedup_vs_plain_fp64": value / plain_value if plain_value else None,
         "e2e": e2e, "roofline": roofline, "clocks": clocks,
+        "tuning": {"table": ctx.tuning_table or "built-in defaults", "knobs": ctx.batch_tuning()},
         "gpu_launches": 2 * args.steps,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -361,6 +361,33 @@ typedef struct krans_request_result {
 int krans_solve_batch(krans_ctx *ctx, int64_t count, const krans_request *reqs,
                       krans_request_result *results, double *device_ms);
 
+/* ---- batched-launch tuning (no reference counterpart) ------------------------
+ * Knobs of krans_solve_batch and of the server's launches, held per context.
+ * The project's autotuner (krans_b200/autotune.py) measures them on probe
+ * batches and caches the winners per device; zero fields keep the built-in
+ * value (in parentheses).
+ *   cluster_min   requests with m + n >= cluster_min run on thread-block
+ *                 clusters, smaller ones on single blocks (16384)
+ *   pair_max      cluster requests with m + n < pair_max run on 2-block
+ *                 clusters of a second launch beside the big clusters (120000)
+ *   cluster_size  blocks per big cluster, 2..16 (8)
+ *   lanes[6]      threads per row of the solvers' SpMV for operands whose mean
+ *                 row length is <= 3, <= 8, <= 16, <= 32, <= 64, > 64
+ *                 (1, 2, 4, 8, 16, 32); powers of two up to 32. Operands whose
+ *                 rows all hold exactly 1, 2 or 4 entries use one thread per
+ *                 row whatever the table says.
+ * The lanes apply to every solve of the context (single and batched); a
+ * request's rounding depends on them, so results are reproducible for a
+ * given table. */
+typedef struct krans_batch_tuning {
+  int64_t cluster_min;
+  int64_t pair_max;
+  int32_t cluster_size;
+  int32_t lanes[6];
+} krans_batch_tuning;
+int krans_ctx_set_batch_tuning(krans_ctx *ctx, const krans_batch_tuning *t);
+int krans_ctx_get_batch_tuning(const krans_ctx *ctx, krans_batch_tuning *t); /* values in effect */
+
 /* ---- serving: continuous batching against an HBM budget ---------------------- */
 typedef struct krans_server krans_server;
 typedef struct krans_server_opts {

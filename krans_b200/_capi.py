@@ -51,6 +51,11 @@ class SpmvTuning(C.Structure):
     _fields_ = [("kernel", C.c_int32), ("rows_per_block", C.c_int32)]
 
 
+class BatchTuning(C.Structure):
+    _fields_ = [("cluster_min", C.c_int64), ("pair_max", C.c_int64), ("cluster_size", C.c_int32),
+                ("lanes", C.c_int32 * 6)]
+
+
 class CyclicOpts(C.Structure):
     _fields_ = [("k", C.c_int64), ("ncv", C.c_int64), ("max_restarts", C.c_int64),
                 ("tol_abs", C.c_double), ("tol_rel", C.c_double),
@@ -128,6 +133,8 @@ SIGNATURES = {
     "krans_ctx_memory_in_use": [P, C.POINTER(C.c_size_t)],
     "krans_ctx_sm_count": [P, C.POINTER(I)],
     "krans_ctx_stream": [P, PP],
+    "krans_ctx_set_batch_tuning": [P, C.POINTER(BatchTuning)],
+    "krans_ctx_get_batch_tuning": [P, C.POINTER(BatchTuning)],
     "krans_csr_create": [P, I64, I64, I64, P, P, P, I, PP],
     "krans_csr_destroy": [P],
     "krans_selftest_barrier_timeout": [P, D, C.POINTER(I), C.POINTER(D)],

@@ -29,13 +29,19 @@ from ._capi import check, load
 class Context:
     """A device, its stream and an optional HBM budget (krans_ctx)."""
 
-    def __init__(self, device: int = 0, hbm_budget: int = 0):
+    def __init__(self, device: int = 0, hbm_budget: int = 0, tuning: bool = True):
+        """tuning: apply the autotuner's table for this device
+        (krans_b200/tuning/<device>.json) when one exists."""
         lib = load()
         h = C.c_void_p()
         check(lib.krans_ctx_create(device, hbm_budget, C.byref(h)), "krans_ctx_create")
         self.h = h
         self.lib = lib
         self.device = device
+        self.tuning_table = None
+        if tuning:
+            from . import autotune
+            self.tuning_table = autotune.apply_cached(self)
 
     def synchronize(self):
         check(self.lib.krans_ctx_synchronize(self.h), "synchronize")
@@ -49,6 +55,19 @@ class Context:
         s = C.c_int()
         check(self.lib.krans_ctx_sm_count(self.h, C.byref(s)))
         return s.value
+
+    def set_batch_tuning(self, cluster_min: int = 0, pair_max: int = 0, cluster_size: int = 0, lanes=None):
+        """Knobs of batched launches (krans_ctx_set_batch_tuning); 0 keeps the
+        built-in value. lanes: 6 threads-per-row entries for mean row lengths
+        <= 3, 8, 16, 32, 64 and above."""
+        t = K.BatchTuning(cluster_min, pair_max, cluster_size, (C.c_int32 * 6)(*(lanes or [0] * 6)))
+        check(self.lib.krans_ctx_set_batch_tuning(self.h, C.byref(t)), "set_batch_tuning")
+
+    def batch_tuning(self) -> dict:
+        t = K.BatchTuning()
+        check(self.lib.krans_ctx_get_batch_tuning(self.h, C.byref(t)), "batch_tuning")
+        return {"cluster_min": int(t.cluster_min), "pair_max": int(t.pair_max),
+                "cluster_size": int(t.cluster_size), "lanes": [int(x) for x in t.lanes]}
 
     def stream_ptr(self) -> int:
         """The context's cudaStream_t (for ordering or timing caller work)."""

@@ -72,25 +72,14 @@ struct BatchLaunch {
     precision = n > 0 ? reqs[0].opts.precision : 0;
     order.resize(n);
     std::iota(order.begin(), order.end(), 0);
-    static const int64_t cluster_min = [] {
-      const char *e = getenv("KRANS_CLUSTER_MIN");
-      return e ? atoll(e) : (int64_t)16384;
-    }();
-    static const int cl_size = [] {
-      const char *e = getenv("KRANS_CLUSTER_SIZE");
-      int v = e ? atoi(e) : 8;
-      return (v >= 2 && v <= 16) ? v : 8;
-    }();
-    csize = cl_size;
+    const int64_t cluster_min = ctx->tune.cluster_min;
+    const int64_t pair_max = ctx->tune.pair_max;
+    csize = ctx->tune.cluster_size;
     // Size classes (by m + n only, so a request runs on the same kind of
     // team, with the same rounding, in any batch): big ones on clusters of
     // csize blocks; mid-size ones on 2-block clusters launched next to them
     // on the SMs the big clusters cannot tile (a GPC holds whole clusters
     // only); small ones on single blocks.
-    static const int64_t pair_max = [] {
-      const char *e = getenv("KRANS_PAIR_MAX");
-      return e ? atoll(e) : (int64_t)120000;
-    }();
     const bool mixed_p = precision == KRANS_PREC_MIXED;
     {
       const int maxc = cyclic_batch_cluster_max(mixed_p, csize, ctx->sms, 0);
@@ -125,8 +114,8 @@ struct BatchLaunch {
                    "krans_solve_batch: mixed precision needs matrices created with KRANS_CSR_FP32");
       const krans_mat *A = r.A;
       CyclicRequestDev &q = hreq[pos];
-      q.F = CsrView{A->m, A->n, A->nnz, A->rp, A->ci, A->v, A->v32, A->lanes, A->ulen};
-      q.B = CsrView{A->n, A->m, A->nnz, A->rpT, A->ciT, A->vT, A->vT32, A->lanesT, A->ulenT};
+      q.F = CsrView{A->m, A->n, A->nnz, A->rp, A->ci, A->v, A->v32, tuned_lanes(A->ctx, A->m, A->nnz), A->ulen};
+      q.B = CsrView{A->n, A->m, A->nnz, A->rpT, A->ciT, A->vT, A->vT32, tuned_lanes(A->ctx, A->n, A->nnz), A->ulenT};
       q.o = r.opts;
       q.o.team = KRANS_TEAM_CTA;
       int64_t kt = (r.opts.nullity_known >= 0) ? (int64_t)r.opts.nullity_known : r.opts.k;

@@ -319,6 +319,31 @@ int krans_ctx_sm_count(const krans_ctx *ctx, int *sms) {
   return KRANS_OK;
 }
 
+int krans_ctx_set_batch_tuning(krans_ctx *ctx, const krans_batch_tuning *t) {
+  KR_CHECK_ARG(ctx && t, "krans_ctx_set_batch_tuning: NULL argument");
+  KR_CHECK_ARG(t->cluster_min >= 0 && t->pair_max >= 0, "krans_ctx_set_batch_tuning: negative size threshold");
+  KR_CHECK_ARG(t->cluster_size == 0 || (t->cluster_size >= 2 && t->cluster_size <= 16),
+               "krans_ctx_set_batch_tuning: cluster_size must be 0 or 2..16");
+  for (int b = 0; b < 6; b++)
+    KR_CHECK_ARG(t->lanes[b] == 0 || (t->lanes[b] >= 1 && t->lanes[b] <= 32 && (t->lanes[b] & (t->lanes[b] - 1)) == 0),
+                 "krans_ctx_set_batch_tuning: lanes must be 0 or a power of two up to 32");
+  const krans_batch_tuning def{16384, 120000, 8, {1, 2, 4, 8, 16, 32}};
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  krans_batch_tuning &u = ctx->tune;
+  u.cluster_min = t->cluster_min ? t->cluster_min : def.cluster_min;
+  u.pair_max = t->pair_max ? t->pair_max : def.pair_max;
+  u.cluster_size = t->cluster_size ? t->cluster_size : def.cluster_size;
+  for (int b = 0; b < 6; b++)
+    u.lanes[b] = t->lanes[b] ? t->lanes[b] : def.lanes[b];
+  return KRANS_OK;
+}
+
+int krans_ctx_get_batch_tuning(const krans_ctx *ctx, krans_batch_tuning *t) {
+  KR_CHECK_ARG(ctx && t, "krans_ctx_get_batch_tuning: NULL argument");
+  *t = ctx->tune;
+  return KRANS_OK;
+}
+
 int krans_ctx_stream(const krans_ctx *ctx, void **stream) {
   KR_CHECK_ARG(ctx && stream, "NULL argument");
   *stream = (void *)ctx->stream;

@@ -63,6 +63,7 @@ struct krans_ctx {
   double *d_scalar = nullptr; // device scalars (reductions)
   double *d_partials = nullptr;
   int partial_blocks = 0;
+  krans_batch_tuning tune{16384, 120000, 8, {1, 2, 4, 8, 16, 32}}; // batched-launch knobs in effect
   std::mutex mu;
 };
 
@@ -114,4 +115,13 @@ int spmv_rows_per_block(int64_t rows, int64_t nnz);
 int dev_alloc(krans_ctx *ctx, void **p, size_t bytes);
 void dev_free(krans_ctx *ctx, void *p, size_t bytes);
 int pick_lanes(int64_t rows, int64_t nnz);
+// threads per row of the solvers' SpMV from the context's tuning table
+inline int tuned_lanes(const krans_ctx *ctx, int64_t rows, int64_t nnz) {
+  const double mean = rows > 0 ? (double)nnz / (double)rows : 0.0;
+  const double bound[5] = {3.0, 8.0, 16.0, 32.0, 64.0};
+  int b = 0;
+  while (b < 5 && mean > bound[b])
+    b++;
+  return ctx->tune.lanes[b];
+}
 } // namespace kr

@@ -19,9 +19,9 @@ static size_t cyclic_layout(const CyclicPlan &p, char *base, CyclicDesc *d) { re
 static CsrView view_of(const krans_mat *A, bool trans) {
   CsrView v;
   if (!trans) {
-    v = CsrView{A->m, A->n, A->nnz, A->rp, A->ci, A->v, A->v32, A->lanes, A->ulen};
+    v = CsrView{A->m, A->n, A->nnz, A->rp, A->ci, A->v, A->v32, tuned_lanes(A->ctx, A->m, A->nnz), A->ulen};
   } else {
-    v = CsrView{A->n, A->m, A->nnz, A->rpT, A->ciT, A->vT, A->vT32, A->lanesT, A->ulenT};
+    v = CsrView{A->n, A->m, A->nnz, A->rpT, A->ciT, A->vT, A->vT32, tuned_lanes(A->ctx, A->n, A->nnz), A->ulenT};
   }
   return v;
 }

@@ -184,8 +184,8 @@ extern "C" int krans_solve_lobpcg(krans_ctx *ctx, const krans_mat *A, krans_rng 
 
   LobpcgDesc d;
   memset(&d, 0, sizeof d);
-  d.F = CsrView{A->m, A->n, A->nnz, A->rp, A->ci, A->v, A->v32, A->lanes, A->ulen};
-  d.B = CsrView{A->n, A->m, A->nnz, A->rpT, A->ciT, A->vT, A->vT32, A->lanesT, A->ulenT};
+  d.F = CsrView{A->m, A->n, A->nnz, A->rp, A->ci, A->v, A->v32, tuned_lanes(A->ctx, A->m, A->nnz), A->ulen};
+  d.B = CsrView{A->n, A->m, A->nnz, A->rpT, A->ciT, A->vT, A->vT32, tuned_lanes(A->ctx, A->n, A->nnz), A->ulenT};
   d.o = o;
   d.k_target = k_target;
   d.bs = bs;
