@@ -333,13 +333,18 @@ int krans_solve_lobpcg(krans_ctx *ctx, const krans_mat *A, krans_rng *rng,
                        double *resid_out, krans_lobpcg_result *result);
 
 /* ---- batched solves: many independent requests in one persistent launch --- */
+#define KRANS_SOLVER_CYCLIC 0 /* find_nullspace_cyclic_lanczos_ex */
+#define KRANS_SOLVER_LOBPCG 1 /* find_nullspace_lobpcg_ex (served requests) */
 typedef struct krans_request {
   const krans_mat *A;        /* matrix of this request */
-  krans_cyclic_opts opts;    /* per-request options (k, tolerances, precision) */
+  krans_cyclic_opts opts;    /* options of a cyclic request (k, tolerances, precision) */
   uint32_t seed;             /* RNG seed of the request's own stream */
   int32_t rng_mode;          /* KRANS_RNG_PHILOX or KRANS_RNG_MT19937 */
-  double *basis_out;         /* device or host? see krans_solve_batch */
+  double *basis_out;         /* DEVICE pointer: basis_capacity x cols(A) doubles, row i = vector i */
   int64_t basis_capacity;    /* vectors that fit in basis_out */
+  int32_t solver;            /* KRANS_SOLVER_CYCLIC; KRANS_SOLVER_LOBPCG for krans_submit only */
+  int32_t reserved;
+  krans_lobpcg_opts lobpcg;  /* options of a LOBPCG request (FP64; its nev / nullity_known set the target) */
 } krans_request;
 
 typedef struct krans_request_result {
@@ -353,6 +358,7 @@ typedef struct krans_request_result {
   double algo_bytes;
   double queue_ms, device_ms, latency_ms; /* see krans_solve_batch / krans_poll */
   double phase_ms[4];        /* device time in Golub-Kahan+reorth, tiny SVD, CG polish, rest */
+  int64_t launch_id;         /* server: sequence number of the launch that ran the request */
 } krans_request_result;
 
 /* Solve `count` cyclic requests in one persistent launch (one thread block
@@ -401,7 +407,15 @@ int krans_server_opts_init(krans_server_opts *o);
 int krans_server_create(krans_ctx *ctx, const krans_server_opts *opts, krans_server **out);
 int krans_server_destroy(krans_server *s);
 /* Queue a request; the server copies the descriptor (A must stay alive until
- * the ticket completes). basis_out is a device pointer as in krans_request. */
+ * the ticket completes). basis_out is a device pointer as in krans_request.
+ * Cyclic requests join a running persistent launch when one has a free team
+ * of their size class: the launch stays resident while requests keep
+ * arriving (its teams leave after 20 ms without work) and leaves 20 SMs free
+ * for other work; a request that does not fit it (another precision, a
+ * larger workspace than its slots) starts the next launch. LOBPCG requests
+ * run one per launch, on one thread block (m + n below the context's
+ * cluster_min) or on a cluster of up to 4 blocks, FP64; their result reports
+ * LOBPCG iterations in `restarts` and locked vectors in `krylov_steps_total`. */
 int krans_submit(krans_server *s, const krans_request *req, uint64_t *ticket);
 /* status: 0 queued, 1 running, 2 done, 3 failed, 4 cancelled */
 int krans_poll(krans_server *s, uint64_t ticket, int *status, krans_request_result *result);

@@ -31,6 +31,8 @@ KRANS_FMT_IJA = 2
 KRANS_TEAM_AUTO = 0
 KRANS_TEAM_CTA = 1
 KRANS_TEAM_GRID = 2
+KRANS_SOLVER_CYCLIC = 0
+KRANS_SOLVER_LOBPCG = 1
 KRANS_SPMV_AUTO = 0
 KRANS_SPMV_ROWTILE = 1
 KRANS_SPMV_UNIFORM = 2
@@ -99,7 +101,8 @@ class LobpcgResultC(C.Structure):
 
 class Request(C.Structure):
     _fields_ = [("A", C.c_void_p), ("opts", CyclicOpts), ("seed", C.c_uint32),
-                ("rng_mode", C.c_int32), ("basis_out", C.c_void_p), ("basis_capacity", C.c_int64)]
+                ("rng_mode", C.c_int32), ("basis_out", C.c_void_p), ("basis_capacity", C.c_int64),
+                ("solver", C.c_int32), ("reserved", C.c_int32), ("lobpcg", LobpcgOpts)]
 
 
 class RequestResult(C.Structure):
@@ -109,7 +112,7 @@ class RequestResult(C.Structure):
                 ("spmv", C.c_int64), ("spmvT", C.c_int64), ("frob_norm_est", C.c_double),
                 ("max_residual", C.c_double), ("algo_bytes", C.c_double),
                 ("queue_ms", C.c_double), ("device_ms", C.c_double), ("latency_ms", C.c_double),
-                ("phase_ms", C.c_double * 4)]
+                ("phase_ms", C.c_double * 4), ("launch_id", C.c_int64)]
 
 
 class ServerOpts(C.Structure):

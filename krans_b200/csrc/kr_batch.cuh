@@ -26,6 +26,69 @@ template <class Team> KR_DEV double team_max_residual(Team &tm, const CsrView &F
 
 extern __shared__ __align__(16) char kr_dyn_smem[];
 
+// Index of the next request of queue `which` (0 large, 1 mid, 2 small) for
+// this team, or -1 when there is none. A closed launch (feed == nullptr)
+// hands out 0 .. count-1. An open launch hands out what the host has
+// published so far, claiming an index only once it is published; a team that
+// finds nothing sleeps between looks until the host publishes more, closes
+// the launch, or feed->idle_ns pass, and then leaves. Every wait is bounded.
+KR_DEV int take_request(int *queue, int count, const LaunchFeed *feed, int which) {
+  if (!feed) {
+    const int it = atomicAdd(queue, 1);
+    return it < count ? it : -1;
+  }
+  const uint64_t t0 = globaltimer_ns();
+  unsigned nap = 256;
+  for (;;) {
+    const int closed = *(volatile const int32_t *)&feed->closed;
+    const int pub = *(volatile const int32_t *)&feed->published[which];
+    int q = *(volatile int *)queue;
+    while (q < pub) {
+      const int got = atomicCAS(queue, q, q + 1);
+      if (got == q)
+        return q;
+      q = got;
+    }
+    if (closed) // read before `published`: nothing more can come
+      return -1;
+    if (globaltimer_ns() - t0 > feed->idle_ns)
+      return -1;
+    __nanosleep(nap);
+    if (nap < 16384)
+      nap *= 2;
+  }
+}
+
+// Copy of request descriptor `src` in this block's shared memory, read
+// through L2 (an open launch's descriptors are written by the host after the
+// launch started, so a line cached in L1 from a neighbouring descriptor may be
+// stale). Called by every thread of the block.
+KR_DEV void load_request(CyclicRequestDev *dst, const CyclicRequestDev *src) {
+  static_assert(sizeof(CyclicRequestDev) % 8 == 0, "descriptor size");
+  const unsigned long long *s8 = reinterpret_cast<const unsigned long long *>(src);
+  unsigned long long *d8 = reinterpret_cast<unsigned long long *>(dst);
+  for (int i = threadIdx.x; i < (int)(sizeof(CyclicRequestDev) / 8); i += blockDim.x)
+    d8[i] = __ldcg(s8 + i);
+  __syncthreads();
+}
+
+// Open launches: copy a finished request's result to its host-mapped
+// completion record, then raise its flag (leader thread only).
+KR_DEV void publish_done(const CyclicRequestDev &rq) {
+  if (!rq.done)
+    return;
+  static_assert(sizeof(CyclicDevResult) % 8 == 0, "result size");
+  HostDone *h = rq.done;
+  const volatile unsigned long long *src = reinterpret_cast<const volatile unsigned long long *>(rq.res);
+  volatile unsigned long long *dst = reinterpret_cast<volatile unsigned long long *>(&h->res);
+  for (int i = 0; i < (int)(sizeof(CyclicDevResult) / 8); i++)
+    dst[i] = src[i];
+  h->max_resid = *(volatile double *)rq.max_resid;
+  h->status = *(volatile int32_t *)rq.status;
+  __threadfence_system();
+  *(volatile int32_t *)&h->done = 1;
+}
+
 // One request on one thread block, with its workspace laid out in `slot`.
 template <class KT>
 __device__ __noinline__ void run_cta_request(TeamShared *sh, CyclicDesc *dp, const CyclicRequestDev &rq,
@@ -68,8 +131,10 @@ __device__ __noinline__ void run_cta_request(TeamShared *sh, CyclicDesc *dp, con
     if (threadIdx.x == 0)
       *rq.max_resid = mr;
   }
-  if (threadIdx.x == 0)
+  if (threadIdx.x == 0) {
     rq.res->t_end = globaltimer_ns();
+    publish_done(rq);
+  }
   __syncthreads();
 }
 
@@ -78,20 +143,23 @@ __device__ __noinline__ void run_cta_request(TeamShared *sh, CyclicDesc *dp, con
 template <class KT>
 __global__ void __launch_bounds__(512, KR_BATCH_MIN_BLOCKS) cyclic_batch_kernel(const CyclicRequestDev *reqs,
                                                                                int count, int *queue, char *ws,
-                                                                               size_t ws_stride) {
+                                                                               size_t ws_stride,
+                                                                               const LaunchFeed *feed) {
   __shared__ TeamShared sh;
   __shared__ CyclicDesc d;
+  __shared__ CyclicRequestDev rq;
   __shared__ int s_item;
   char *slot = ws + (size_t)blockIdx.x * ws_stride;
   for (;;) {
     if (threadIdx.x == 0)
-      s_item = atomicAdd(queue, 1);
+      s_item = take_request(queue, count, feed, 2);
     __syncthreads();
     const int item = s_item;
     __syncthreads();
-    if (item >= count)
+    if (item < 0)
       break;
-    run_cta_request<KT>(&sh, &d, reqs[item], slot);
+    load_request(&rq, reqs + item);
+    run_cta_request<KT>(&sh, &d, rq, slot);
   }
 }
 
@@ -105,9 +173,11 @@ template <class KT>
 __global__ void __launch_bounds__(512, KR_BATCH_MIN_BLOCKS)
     cyclic_batch_cluster_kernel(const CyclicRequestDev *reqs_large, int n_large, int *queue_large, char *ws_large,
                                 size_t stride_large, const CyclicRequestDev *reqs_small, int n_small,
-                                int *queue_small, char *ws_small, size_t stride_small) {
+                                int *queue_small, char *ws_small, size_t stride_small, const LaunchFeed *feed,
+                                int feed_large) {
   __shared__ TeamShared sh;
   __shared__ CyclicDesc d;
+  __shared__ CyclicRequestDev rq;
   __shared__ int s_item;
   cooperative_groups::cluster_group cl = cooperative_groups::this_cluster();
   const unsigned rank = cl.block_rank(), csize = cl.num_blocks();
@@ -115,13 +185,13 @@ __global__ void __launch_bounds__(512, KR_BATCH_MIN_BLOCKS)
   int cbuf = 0;
   for (;;) {
     if (rank == 0 && threadIdx.x == 0)
-      s_item = atomicAdd(queue_large, 1);
+      s_item = take_request(queue_large, n_large, feed, feed_large);
     cl.sync();
     const int item = *cl.map_shared_rank(&s_item, 0);
     cl.sync();
-    if (item >= n_large)
+    if (item < 0)
       break;
-    const CyclicRequestDev &rq = reqs_large[item];
+    load_request(&rq, reqs_large + item);
     if (threadIdx.x == 0) {
       memset(&d, 0, sizeof d);
       cyclic_carve(rq.plan, slot, &d);
@@ -152,21 +222,24 @@ __global__ void __launch_bounds__(512, KR_BATCH_MIN_BLOCKS)
         *rq.max_resid = mr;
       cbuf = tm.cbuf;
     }
-    if (rank == 0 && threadIdx.x == 0)
+    if (rank == 0 && threadIdx.x == 0) {
       rq.res->t_end = globaltimer_ns();
+      publish_done(rq);
+    }
     cl.sync();
   }
   // small requests, block by block (no cluster-wide synchronisation below)
   char *cslot = ws_small + (size_t)blockIdx.x * stride_small;
   for (;;) {
     if (threadIdx.x == 0)
-      s_item = atomicAdd(queue_small, 1);
+      s_item = take_request(queue_small, n_small, feed, 2);
     __syncthreads();
     const int item = s_item;
     __syncthreads();
-    if (item >= n_small)
+    if (item < 0)
       break;
-    run_cta_request<KT>(&sh, &d, reqs_small[item], cslot);
+    load_request(&rq, reqs_small + item);
+    run_cta_request<KT>(&sh, &d, rq, cslot);
   }
 }
 

@@ -294,9 +294,9 @@ __host__ __device__ constexpr size_t gram_tiled_smem_bytes() { return (size_t)3 
 template <class Team>
 KR_DEV void team_gram_sym_tiled(Team &tm, int64_t n, const double *Z, const double *AZ, int64_t ld, int p,
                                 double *S, double *G, double *part) {
-  extern __shared__ __align__(16) double kr_dyn_smem[];
+  extern __shared__ __align__(16) double kr_gemm_smem[];
   typedef double Panel[KR_GP + 1];
-  Panel *sA = reinterpret_cast<Panel *>(kr_dyn_smem);
+  Panel *sA = reinterpret_cast<Panel *>(kr_gemm_smem);
   Panel *sB = sA + KR_GT, *sC = sB + KR_GT;
   const bool withG = AZ != nullptr;
   const int tp = (p + KR_GT - 1) / KR_GT, tu = tp * (tp + 1) / 2;
@@ -453,9 +453,9 @@ __host__ __device__ constexpr size_t gemm_nn_smem_bytes() { return (size_t)(KR_N
 template <class Team>
 KR_DEV void team_gemm_nn(Team &tm, int64_t n, const double *Z, int64_t ld, int zc, const double *Y, int ldy,
                          int roff, int q, double *out, bool subtract) {
-  extern __shared__ __align__(16) double kr_dyn_smem[];
-  double(*sZ)[KR_NK + 1] = reinterpret_cast<double(*)[KR_NK + 1]>(kr_dyn_smem);
-  double(*sY)[KR_NK + 1] = reinterpret_cast<double(*)[KR_NK + 1]>(kr_dyn_smem + KR_NT * (KR_NK + 1));
+  extern __shared__ __align__(16) double kr_gemm_smem[];
+  double(*sZ)[KR_NK + 1] = reinterpret_cast<double(*)[KR_NK + 1]>(kr_gemm_smem);
+  double(*sY)[KR_NK + 1] = reinterpret_cast<double(*)[KR_NK + 1]>(kr_gemm_smem + KR_NT * (KR_NK + 1));
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int wr = (wid >> 2) * 16, wc = (wid & 3) * 32; // this warp's 16 x 32 piece
   const int64_t row_tiles = (n + KR_NT - 1) / KR_NT;

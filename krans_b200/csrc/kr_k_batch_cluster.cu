@@ -43,7 +43,8 @@ int cyclic_batch_cluster_max(bool mixed, int csize, int sms, size_t dyn_smem) {
 cudaError_t launch_cyclic_batch_cluster(bool mixed, int nclusters, int csize, size_t dyn_smem, cudaStream_t s,
                                         const CyclicRequestDev *reqs_large, int n_large, int *queue_large,
                                         char *ws_large, size_t stride_large, const CyclicRequestDev *reqs_small,
-                                        int n_small, int *queue_small, char *ws_small, size_t stride_small) {
+                                        int n_small, int *queue_small, char *ws_small, size_t stride_small,
+                                        const LaunchFeed *feed, int feed_large) {
   cudaLaunchAttribute at[1];
   cudaError_t e = cudaFuncSetAttribute(cl_kernel(mixed), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn_smem);
   if (e != cudaSuccess)
@@ -51,9 +52,10 @@ cudaError_t launch_cyclic_batch_cluster(bool mixed, int nclusters, int csize, si
   cudaLaunchConfig_t cfg = cl_config(nclusters, csize, dyn_smem, s, at);
   if (mixed)
     return cudaLaunchKernelEx(&cfg, cyclic_batch_cluster_kernel<float>, reqs_large, n_large, queue_large, ws_large,
-                              stride_large, reqs_small, n_small, queue_small, ws_small, stride_small);
+                              stride_large, reqs_small, n_small, queue_small, ws_small, stride_small, feed,
+                              feed_large);
   return cudaLaunchKernelEx(&cfg, cyclic_batch_cluster_kernel<double>, reqs_large, n_large, queue_large, ws_large,
-                            stride_large, reqs_small, n_small, queue_small, ws_small, stride_small);
+                            stride_large, reqs_small, n_small, queue_small, ws_small, stride_small, feed, feed_large);
 }
 
 } // namespace kr

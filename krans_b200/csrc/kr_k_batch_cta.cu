@@ -16,15 +16,15 @@ int cyclic_batch_cta_per_sm(bool mixed) {
 }
 
 cudaError_t launch_cyclic_batch_cta(bool mixed, int grid, int block, size_t dyn_smem, cudaStream_t s, const CyclicRequestDev *reqs,
-                                    int count, int *queue, char *ws, size_t stride) {
+                                    int count, int *queue, char *ws, size_t stride, const LaunchFeed *feed) {
   const void *k = mixed ? (const void *)cyclic_batch_kernel<float> : (const void *)cyclic_batch_kernel<double>;
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn_smem);
   if (e != cudaSuccess)
     return e;
   if (mixed)
-    cyclic_batch_kernel<float><<<grid, block, dyn_smem, s>>>(reqs, count, queue, ws, stride);
+    cyclic_batch_kernel<float><<<grid, block, dyn_smem, s>>>(reqs, count, queue, ws, stride, feed);
   else
-    cyclic_batch_kernel<double><<<grid, block, dyn_smem, s>>>(reqs, count, queue, ws, stride);
+    cyclic_batch_kernel<double><<<grid, block, dyn_smem, s>>>(reqs, count, queue, ws, stride, feed);
   return cudaGetLastError();
 }
 

@@ -973,6 +973,18 @@ __global__ void __launch_bounds__(512) lobpcg_grid_kernel(LobpcgDesc d) {
 }
 #endif
 
+#ifdef KR_LOBPCG_CLUSTER_KERNEL
+// one solve on a thread-block cluster (served LOBPCG requests)
+__global__ void __launch_bounds__(512) lobpcg_cluster_kernel(const LobpcgDesc *dp) {
+  __shared__ TeamShared sh;
+  const LobpcgDesc &d = *dp;
+  cooperative_groups::cluster_group cl = cooperative_groups::this_cluster();
+  TeamCluster tm{&sh, d.status, 0, 0, cl.block_rank(), cl.num_blocks()};
+  LobpcgSolver<TeamCluster> s(tm, d);
+  s.run();
+}
+#endif
+
 #ifdef KR_LOBPCG_CTA_KERNEL
 __global__ void __launch_bounds__(512) lobpcg_cta_kernel(const LobpcgDesc *dp) {
   __shared__ TeamShared sh;

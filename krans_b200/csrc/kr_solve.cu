@@ -163,7 +163,7 @@ static int run_cyclic(krans_ctx *ctx, const krans_mat *A, bool trans, krans_rng 
                                        cta_cg_smem_bytes(p.ldm, p.ldn) <= cta_smem_cap()
                                            ? cta_cg_smem_bytes(p.ldm, p.ldn)
                                            : 0,
-                                       s, d_req, 1, d_queue, slot, 0);
+                                       s, d_req, 1, d_queue, slot, 0, nullptr);
   if (e == cudaSuccess)
     e = cudaEventRecord(e1, s);
   if (e == cudaSuccess)

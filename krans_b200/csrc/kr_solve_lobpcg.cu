@@ -302,3 +302,236 @@ extern "C" int krans_solve_lobpcg(krans_ctx *ctx, const krans_mat *A, krans_rng 
       resid_out[i] = rs[i];
   return rc;
 }
+
+// ---------------------------------------------------------------------------
+// Served LOBPCG requests (krans_submit with KRANS_SOLVER_LOBPCG): planned,
+// launched on one of the server's streams and polled, without blocking the
+// server's scheduler. One thread block solves requests with m + n below the
+// context's cluster_min, a thread-block cluster the larger ones (the whole-GPU
+// cooperative team would stall every other launch). After the solve, one
+// block computes max ||A u|| of the returned basis.
+// ---------------------------------------------------------------------------
+namespace kr {
+
+cudaError_t launch_lobpcg_cluster(const LobpcgDesc *d_dev, int csize, cudaStream_t s);
+cudaError_t launch_lobpcg_cta(const LobpcgDesc *d_dev, int threads, cudaStream_t s);
+cudaError_t launch_basis_max_residual(const CsrView &F, const double *basis, int64_t ldb, const int64_t *nf,
+                                      double *out, cudaStream_t s);
+
+struct LobpcgAsync {
+  krans_ctx *ctx = nullptr;
+  krans_request req;
+  LobpcgDesc d;
+  int64_t m = 0, n = 0, k_target = 0, bs = 0, pmax = 0;
+  int ncta = 1;
+  bool trivial = false, converged_trivial = false;
+  char *ws = nullptr;
+  size_t bytes = 0, layout_bytes = 0;
+  LobpcgDesc *d_desc = nullptr;
+  RngState *d_rng = nullptr;
+  double *d_mr = nullptr;
+  LobpcgDevResult *h_res = nullptr;
+  double *h_mr = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr, evd = nullptr;
+};
+
+static void seed_state(RngState &s, uint32_t seed, int mode) {
+  memset(&s, 0, sizeof s);
+  s.mt[0] = seed;
+  for (int i = 1; i < 624; i++)
+    s.mt[i] = 1812433253u * (s.mt[i - 1] ^ (s.mt[i - 1] >> 30)) + (uint32_t)i;
+  s.idx = 624;
+  s.philox_key = ((uint64_t)seed << 32) ^ 0x9E3779B97F4A7C15ull;
+  s.mode = mode;
+}
+
+int lobpcg_async_plan(krans_ctx *ctx, const krans_request &r, LobpcgAsync **out, size_t *need) {
+  *out = nullptr;
+  *need = 0;
+  KR_CHECK_ARG(r.A && r.A->ctx == ctx, "krans_submit: request without a matrix of this context");
+  const krans_lobpcg_opts &o = r.lobpcg;
+  KR_CHECK_ARG(o.precision == KRANS_PREC_FP64, "krans_submit: LOBPCG requests run in FP64");
+  auto *a = new LobpcgAsync();
+  a->ctx = ctx;
+  a->req = r;
+  const krans_mat *A = r.A;
+  a->m = A->m;
+  a->n = A->n;
+  const int64_t m = A->m, n = A->n;
+  // k_target rules and argument checks (LOBPCGSolver.cpp:453-476)
+  int64_t k_target = std::max<int64_t>(1, o.nev);
+  if (o.nullity_known >= 0) {
+    if ((int64_t)o.nullity_known > n) {
+      delete a;
+      set_error("LOBPCG: nullity_known > n");
+      return KRANS_ERR_INVALID_ARGUMENT;
+    }
+    k_target = o.nullity_known;
+  }
+  if (o.rank_known >= 0) {
+    const int64_t rk = o.rank_known, implied = n - rk;
+    if (rk > n || (o.nullity_known >= 0 && implied != k_target)) {
+      delete a;
+      set_error(rk > n ? "LOBPCG: rank_known > n" : "LOBPCG: inconsistent rank_known vs nullity_known");
+      return KRANS_ERR_INVALID_ARGUMENT;
+    }
+    if (o.nullity_known < 0)
+      k_target = implied;
+    if (n <= rk) {
+      a->trivial = true;
+      a->converged_trivial = k_target == 0;
+    }
+  }
+  if (n == 0 || m == 0)
+    a->trivial = true;
+  a->k_target = k_target;
+  if (a->trivial) {
+    *out = a;
+    return KRANS_OK;
+  }
+  int64_t bs = o.block_size > 0 ? o.block_size : std::min<int64_t>(16, std::max<int64_t>(1, k_target));
+  bs = std::min<int64_t>(bs, n);
+  if (bs > 128 || k_target > 512 || !r.basis_out || r.basis_capacity < k_target ||
+      o.precond_normal < KRANS_PRECOND_NONE || o.precond_normal > KRANS_PRECOND_SD || o.precond_steps < 1 ||
+      o.precond_steps > 1000) {
+    delete a;
+    set_error("krans_submit: LOBPCG request needs block_size <= 128, at most 512 vectors, basis_out of "
+              "capacity >= its target and a KRANS_PRECOND_* preconditioner");
+    return KRANS_ERR_INVALID_ARGUMENT;
+  }
+  a->bs = bs;
+  a->pmax = std::max<int64_t>(3 * bs, 2 * k_target + 2);
+  const bool cluster = (m + n) >= ctx->tune.cluster_min;
+  a->ncta = cluster ? std::min(4, std::max(2, ctx->tune.cluster_size)) : 1;
+  LobpcgDesc &d = a->d;
+  memset(&d, 0, sizeof d);
+  d.F = CsrView{A->m, A->n, A->nnz, A->rp, A->ci, A->v, A->v32, tuned_lanes(ctx, A->m, A->nnz), A->ulen};
+  d.B = CsrView{A->n, A->m, A->nnz, A->rpT, A->ciT, A->vT, A->vT32, tuned_lanes(ctx, A->n, A->nnz), A->ulenT};
+  d.o = o;
+  d.o.team = cluster ? KRANS_TEAM_GRID : KRANS_TEAM_CTA; // informational only
+  d.k_target = k_target;
+  d.bs = bs;
+  d.guards = (bs == 1) ? 0 : std::min<int64_t>((int64_t)((1.0 - o.restart) * (double)bs + 0.45), bs - 1);
+  d.n_initial = 0;
+  a->layout_bytes = lobpcg_layout(m, n, bs, k_target, a->pmax, a->ncta, nullptr, nullptr);
+  a->bytes = kr_round_up((int64_t)a->layout_bytes, 256) + kr_round_up(sizeof(LobpcgDesc), 256) +
+             kr_round_up(sizeof(RngState), 256) + 256;
+  *need = a->bytes;
+  *out = a;
+  return KRANS_OK;
+}
+
+int lobpcg_async_launch(LobpcgAsync *a, cudaStream_t s) {
+  if (a->trivial)
+    return KRANS_OK;
+  int rc = dev_alloc(a->ctx, (void **)&a->ws, a->bytes);
+  if (rc != KRANS_OK)
+    return rc;
+  char *p = a->ws;
+  LobpcgDesc &d = a->d;
+  d.rng = nullptr;
+  lobpcg_layout(a->m, a->n, a->bs, a->k_target, a->pmax, a->ncta, p, &d);
+  p += kr_round_up((int64_t)a->layout_bytes, 256);
+  a->d_desc = reinterpret_cast<LobpcgDesc *>(p);
+  p += kr_round_up(sizeof(LobpcgDesc), 256);
+  a->d_rng = reinterpret_cast<RngState *>(p);
+  d.rng = a->d_rng;
+  a->d_mr = d.dflag + 3; // a spare slot of the workspace's scalar flags
+  RngState st;
+  seed_state(st, a->req.seed ? a->req.seed : 0x9E3779B9u, a->req.rng_mode);
+  cudaError_t e = cudaMallocHost(&a->h_res, sizeof(LobpcgDevResult));
+  if (e == cudaSuccess)
+    e = cudaMallocHost(&a->h_mr, sizeof(double));
+  if (e == cudaSuccess)
+    e = cudaEventCreate(&a->ev0);
+  if (e == cudaSuccess)
+    e = cudaEventCreate(&a->ev1);
+  if (e == cudaSuccess)
+    e = cudaEventCreateWithFlags(&a->evd, cudaEventDisableTiming);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(a->d_rng, &st, sizeof st, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(a->d_desc, &d, sizeof d, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess)
+    e = cudaMemsetAsync(d.status, 0, 4, s);
+  if (e == cudaSuccess)
+    e = cudaMemsetAsync(d.gb, 0, sizeof(GridBarrierState), s);
+  if (e == cudaSuccess)
+    e = cudaMemsetAsync(d.res, 0, sizeof(LobpcgDevResult), s);
+  if (e == cudaSuccess)
+    e = cudaMemsetAsync(a->d_mr, 0, sizeof(double), s);
+  if (e == cudaSuccess)
+    e = cudaStreamSynchronize(s); // the host copies above came from this stack frame
+  if (e == cudaSuccess)
+    e = cudaEventRecord(a->ev0, s);
+  if (e == cudaSuccess)
+    e = a->ncta > 1 ? launch_lobpcg_cluster(a->d_desc, a->ncta, s) : launch_lobpcg_cta(a->d_desc, 512, s);
+  if (e == cudaSuccess)
+    e = cudaEventRecord(a->ev1, s);
+  if (e == cudaSuccess)
+    e = launch_basis_max_residual(d.F, d.RN, d.ldn, &d.res->n_right, a->d_mr, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(a->h_res, d.res, sizeof(LobpcgDevResult), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(a->h_mr, a->d_mr, sizeof(double), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess && a->k_target > 0)
+    e = cudaMemcpy2DAsync(a->req.basis_out, (size_t)a->n * 8, d.RN, (size_t)d.ldn * 8, (size_t)a->n * 8,
+                          (size_t)a->k_target, cudaMemcpyDeviceToDevice, s);
+  if (e == cudaSuccess)
+    e = cudaEventRecord(a->evd, s);
+  if (e != cudaSuccess)
+    return cuda_fail(e, "served LOBPCG launch", __FILE__, __LINE__);
+  return KRANS_OK;
+}
+
+bool lobpcg_async_done(const LobpcgAsync *a) { return a->trivial || cudaEventQuery(a->evd) == cudaSuccess; }
+
+void lobpcg_async_finish(const LobpcgAsync *a, krans_request_result *out) {
+  memset(out, 0, sizeof *out);
+  if (a->trivial) {
+    out->converged_to_target = a->converged_trivial ? 1 : 0;
+    return;
+  }
+  const LobpcgDevResult &R = *a->h_res;
+  out->status = R.status;
+  if (out->status == KRANS_OK && R.err_code != kLobErrNone) {
+    out->status = KRANS_ERR_RUNTIME;
+    set_error("%s", lobpcg_err_msg(R.err_code));
+  }
+  out->converged_to_target = R.converged;
+  out->n_right = R.n_right;
+  out->restarts = R.iters;
+  out->krylov_steps_total = R.locked;
+  out->spmv = R.spmv;
+  out->spmvT = R.spmvT;
+  out->frob_norm_est = R.frob;
+  out->max_residual = *a->h_mr;
+  out->algo_bytes = R.bytes;
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, a->ev0, a->ev1);
+  out->device_ms = ms;
+  out->phase_ms[0] = R.phase_ms[0];
+  out->phase_ms[1] = R.phase_ms[1] + R.phase_ms[2];
+  out->phase_ms[2] = R.phase_ms[3];
+  out->phase_ms[3] = R.phase_ms[4];
+}
+
+void lobpcg_async_release(LobpcgAsync *a) {
+  if (!a)
+    return;
+  if (a->ws)
+    dev_free(a->ctx, a->ws, a->bytes);
+  if (a->h_res)
+    cudaFreeHost(a->h_res);
+  if (a->h_mr)
+    cudaFreeHost(a->h_mr);
+  if (a->ev0)
+    cudaEventDestroy(a->ev0);
+  if (a->ev1)
+    cudaEventDestroy(a->ev1);
+  if (a->evd)
+    cudaEventDestroy(a->evd);
+  delete a;
+}
+
+} // namespace kr

@@ -169,6 +169,24 @@ __host__ __device__ inline size_t cyclic_carve(const CyclicPlan &p, char *base, 
   return c.off + 256;
 }
 
+// Completion record of one request of an open launch, in host-mapped pinned
+// memory: the team copies its result here and then sets `done`, which the
+// host polls while the launch keeps running.
+struct HostDone {
+  CyclicDevResult res;
+  double max_resid;
+  int32_t status;
+  int32_t done;
+};
+
+// The requests an open launch may take, published by the host while it runs
+// (host-mapped pinned memory: the host writes, the device only reads).
+struct LaunchFeed {
+  int32_t published[3]; // requests published to the large, mid and small queues
+  int32_t closed;       // nonzero: the host publishes no more requests to this launch
+  uint64_t idle_ns;     // a team that finds no request for this long leaves the launch
+};
+
 struct CyclicRequestDev {
   CsrView F, B;
   krans_cyclic_opts o;
@@ -179,6 +197,7 @@ struct CyclicRequestDev {
   int32_t *status;
   double *max_resid;
   const double *initial_right; // start vector y0 or nullptr
+  HostDone *done;              // open launches: completion record (else nullptr)
   int32_t trivial;   // reference early exit: nothing to compute
   int32_t trans_run; // 1: the run is on A^T (left null space)
 };
@@ -241,12 +260,13 @@ int cyclic_grid_blocks(krans_ctx *ctx, bool mixed, int threads);
 cudaError_t launch_cyclic_grid(bool mixed, const CyclicDesc &d, int blocks, int threads, cudaStream_t s);
 int cyclic_batch_cta_per_sm(bool mixed);
 cudaError_t launch_cyclic_batch_cta(bool mixed, int grid, int block, size_t dyn_smem, cudaStream_t s, const CyclicRequestDev *reqs, int count,
-                                    int *queue, char *ws, size_t stride);
+                                    int *queue, char *ws, size_t stride, const LaunchFeed *feed);
 int cyclic_batch_cluster_max(bool mixed, int csize, int sms, size_t dyn_smem);
 cudaError_t launch_cyclic_batch_cluster(bool mixed, int nclusters, int csize, size_t dyn_smem, cudaStream_t s,
                                         const CyclicRequestDev *reqs_large, int n_large, int *queue_large,
                                         char *ws_large, size_t stride_large, const CyclicRequestDev *reqs_small,
-                                        int n_small, int *queue_small, char *ws_small, size_t stride_small);
+                                        int n_small, int *queue_small, char *ws_small, size_t stride_small,
+                                        const LaunchFeed *feed, int feed_large);
 int lobpcg_grid_blocks(krans_ctx *ctx, int threads);
 cudaError_t launch_lobpcg(bool grid, const LobpcgDesc &d, const LobpcgDesc *d_dev, int blocks, int threads,
                           cudaStream_t s);

@@ -1,9 +1,10 @@
 """Batched solves and the continuous-batching server (Python mirror of
 krans_solve_batch / krans_server_* in include/krans_cuda.h).
 
-A request is one cyclic null-space solve of its own matrix with its own
-options and RNG stream; its basis is written to a device buffer owned by the
-request object.
+A request is one null-space solve of its own matrix with its own options
+and RNG stream: cyclic Lanczos (batched launches and the server) or LOBPCG
+(the server); its basis is written to a device buffer owned by the request
+object.
 """
 from __future__ import annotations
 
@@ -16,23 +17,37 @@ import numpy as np
 
 from . import _capi as K
 from ._capi import check
-from .api import Context, CudaCsrMatrixAdapter, CudaVectorAdapter, CyclicLanczosOptions
+from .api import Context, CudaCsrMatrixAdapter, CudaVectorAdapter, CyclicLanczosOptions, LOBPCGOptions
 
 STATUS = {0: "queued", 1: "running", 2: "done", 3: "failed", 4: "cancelled"}
 
 
 @dataclass
 class SolveRequest:
+    """opts: CyclicLanczosOptions (solver "cyclic") or LOBPCGOptions (solver
+    "lobpcg", served requests only; FP64). For LOBPCG results, `restarts`
+    counts LOBPCG iterations and `krylov_steps_total` the locked vectors."""
     A: CudaCsrMatrixAdapter
-    opts: CyclicLanczosOptions
+    opts: object
     seed: int = 1
     rng_mode: str = "philox"
     buf: Optional[CudaVectorAdapter] = None
     result: Optional[K.RequestResult] = None
     ticket: int = 0
 
+    @property
+    def solver(self) -> str:
+        return "lobpcg" if isinstance(self.opts, LOBPCGOptions) else "cyclic"
+
     def k_target(self) -> int:
-        return self.opts.nullity_known if self.opts.nullity_known >= 0 else self.opts.k
+        o = self.opts
+        if self.solver == "lobpcg":
+            if o.nullity_known >= 0:
+                return o.nullity_known
+            if o.rank_known >= 0:
+                return max(0, self.A.n - o.rank_known)
+            return max(1, o.nev)
+        return o.nullity_known if o.nullity_known >= 0 else o.k
 
     def to_c(self, ctx: Context) -> K.Request:
         kt = max(self.k_target(), 1)
@@ -40,7 +55,13 @@ class SolveRequest:
             self.buf = CudaVectorAdapter(ctx, kt * self.A.n)
         r = K.Request()
         r.A = self.A.h
-        r.opts = self.opts.to_c()
+        if self.solver == "lobpcg":
+            r.solver = K.KRANS_SOLVER_LOBPCG
+            r.lobpcg = self.opts.to_c()
+            K.load().krans_cyclic_opts_init(C.byref(r.opts))
+        else:
+            r.solver = K.KRANS_SOLVER_CYCLIC
+            r.opts = self.opts.to_c()
         r.seed = self.seed & 0xFFFFFFFF
         r.rng_mode = {"mt19937": K.KRANS_RNG_MT19937, "philox": K.KRANS_RNG_PHILOX}[self.rng_mode]
         r.basis_out = self.buf.device_ptr()
