@@ -783,41 +783,69 @@ def run_spmv(args):
     return 0
 
 
-def serving_pool(P, nnz_lo, nnz_hi, seed=7):
-    """Request matrices of the serving stream: shift and incidence operators
-    (mean degree 6, as in the batched workload), incidence of mean degree 8 and
-    planted kernels, nnz log-uniform in [nnz_lo, nnz_hi]."""
+def serving_pool(P, nnz_lo, nnz_hi, kmax=64, seed=7):
+    """Request matrices of the serving stream: each draws one of three
+    generators in turn, nnz log-uniform in [nnz_lo, nnz_hi]:
+      graph incidence, mean degree 8, k components (k uniform in 1..kmax),
+          solved by block LOBPCG (the large-LOBPCG workload's generator)
+      planted kernel A = [B | B W], 8 entries per row of B, k planted
+          (1..kmax), cyclic Lanczos in mixed precision (the planted workload's)
+      the batched workload's: a shift operator with N = k (1..16) or an
+          incidence matrix of mean degree 6 with k components (1..16), cyclic,
+          mixed precision.
+    Returns [(instance, solver)]."""
     from krans_b200 import generators as G
     out = []
     for i in range(P):
         r = np.random.Generator(np.random.PCG64([seed, i]))
         nnz = float(np.exp(r.uniform(np.log(nnz_lo), np.log(nnz_hi))))
-        kind = i % 4
+        kind = i % 3
         if kind == 0:
-            N = int(r.integers(1, 17))
-            out.append(G.shift_operator(max(int(nnz / 2), 64), N, float(r.uniform(0.3, 0.9)), kernel=False))
-        elif kind in (1, 2):
-            deg = 6.0 if kind == 1 else 8.0
-            comps = int(r.integers(1, 17))
-            out.append(G.graph_incidence(max(int(nnz / deg), 4 * comps), comps, deg,
-                                         seed=int(r.integers(1 << 31)), kernel=False))
+            k = int(r.integers(1, kmax + 1))
+            nv = max(int(nnz / 8), 16 * k)
+            out.append((G.graph_incidence(nv, k, 8.0, seed=int(r.integers(1 << 31)), kernel=False), "lobpcg"))
+        elif kind == 1:
+            k = int(r.integers(1, kmax + 1))
+            m = max(int(nnz / 8), 64 * k)
+            out.append((G.planted_kernel(m, max(2 * m // 3, 8 * k), k, seed=int(r.integers(1 << 31)), kernel=False),
+                        "cyclic"))
         else:
-            k = int(r.integers(1, 9))
-            nk = max(int(nnz / 13), 64)
-            out.append(G.planted_kernel(int(1.5 * nk), nk, k, seed=int(r.integers(1 << 31)), kernel=False))
+            k = int(r.integers(1, 17))
+            if r.random() < 0.5:
+                out.append((G.shift_operator(max(int(nnz / 2), 4 * k), k, float(r.uniform(0.3, 0.9)), kernel=False),
+                            "cyclic"))
+            else:
+                out.append((G.graph_incidence(max(int(nnz / 6), 4 * k), k, 6.0, seed=int(r.integers(1 << 31)),
+                                              kernel=False), "cyclic"))
     return out
 
 
-def _stream(ctx, pool, mats, rate, seconds, precision, max_inflight, max_batch, seed):
+def serving_opts(kb, inst, solver, precision):
+    L = lower_norm_bound(inst.A)
+    k = inst.k
+    if solver == "lobpcg":
+        return kb.LOBPCGOptions(nev=k, block_size=min(128, max(k + 4, (3 * k + 1) // 2)), tol_abs=1e-12 * L,
+                                tol_rel=0.0, max_iters=1000)
+    ncv = min(256, max(48, 3 * k))
+    return kb.CyclicLanczosOptions(k=k, ncv=ncv, max_restarts=400, tol_abs=1e-12 * L, tol_rel=0.0, cg_maxit=1000,
+                                   precision=kb.Precision(precision))
+
+
+def _stream(ctx, pool, mats, bounds, rate, seconds, precision, max_inflight, max_batch, seed, budget):
     """Poisson arrivals at `rate`/s for `seconds`; each request draws a pool
-    matrix. Requests still unfinished when the window closes are cancelled
-    (queued) or drained (running) and do not count as completed."""
+    matrix. When the window closes, every unfinished request is cancelled
+    (queued ones at once, running ones at their team's next status check) and
+    does not count as completed. Latency = submit -> done, queueing included."""
     import krans_b200 as kb
     from krans_b200.serving import Server, SolveRequest
+    from krans_b200._capi import KransError
     rng = np.random.default_rng(seed)
-    srv = Server(ctx, max_inflight=max_inflight, max_batch=max_batch)
+    opts = {"cyclic": {}, "lobpcg": {}}
+    for i, (inst, solver) in enumerate(pool):
+        opts[solver][i] = serving_opts(kb, inst, solver, precision)
+    srv = Server(ctx, hbm_budget=budget, max_inflight=max_inflight, max_batch=max_batch)
     pending = {}
-    lat = []
+    lat, lat_kind = [], {"cyclic": [], "lobpcg": []}
     done = ok = offered = 0
     t0 = time.perf_counter()
     nxt = rng.exponential(1.0 / rate)
@@ -827,69 +855,74 @@ def _stream(ctx, pool, mats, rate, seconds, precision, max_inflight, max_batch, 
             break
         while nxt <= now:
             i = int(rng.integers(len(pool)))
-            inst = pool[i]
-            o = kb.CyclicLanczosOptions(k=inst.k, tol_abs=1e-12 * lower_norm_bound(inst.A), tol_rel=0.0,
-                                        cg_maxit=1000, precision=kb.Precision(precision))
-            rq = SolveRequest(mats[i], o, seed=offered + 1)
-            pending[srv.submit(rq)] = rq
+            inst, solver = pool[i]
+            rq = SolveRequest(mats[i], opts[solver][i], seed=offered + 1, keep_basis=False)
+            pending[srv.submit(rq)] = (rq, i, solver)
             offered += 1
             nxt += rng.exponential(1.0 / rate)
-        for t in list(pending):
+        for t in srv.completed():
             st, res = srv.poll(t)
-            if st in ("done", "failed"):
-                pending.pop(t)
+            if t in pending and st in ("done", "failed"):
+                rq, i, solver = pending.pop(t)
                 done += 1
-                ok += int(st == "done" and res.converged_to_target)
+                good = st == "done" and res.converged_to_target and res.max_residual <= bounds[i]
+                ok += int(good)
                 lat.append(res.latency_ms)
-        time.sleep(0.002)
+                lat_kind[solver].append(res.latency_ms)
+        time.sleep(0.001)
     elapsed = time.perf_counter() - t0
     unfinished = len(pending)
-    from krans_b200._capi import KransError
     for t in list(pending):
         try:
-            srv.cancel(t)  # still queued
+            srv.cancel(t)
         except KransError:
-            pass           # already running: drained below
-    srv.drain(600.0)
+            pass  # finished meanwhile
+    srv.drain(900.0)
     srv.close()
-    return {"offered": offered, "completed": done, "converged": ok, "window_s": elapsed,
+    return {"offered": offered, "offered_rate": rate, "completed": done, "met_1e-12": ok, "window_s": elapsed,
             "sustained_solves_per_s": done / elapsed,
-            "p50_ms": percentile(lat, 50), "p99_ms": percentile(lat, 99), "unfinished": unfinished}
+            "p50_ms": percentile(lat, 50), "p99_ms": percentile(lat, 99),
+            "p50_ms_cyclic": percentile(lat_kind["cyclic"], 50), "p50_ms_lobpcg": percentile(lat_kind["lobpcg"], 50),
+            "completed_lobpcg": len(lat_kind["lobpcg"]), "unfinished_cancelled": unfinished}
 
 
 def run_serving(args):
     """Serving stream: Poisson arrivals into the continuous-batching server
-    (mixed precision, HBM budget 150 GB) at an offered load below its measured
-    capacity and at an oversubscribed one; the plain FP64 one-at-a-time path
-    on the same stream as the baseline."""
+    (HBM budget 150 GB) at the stated rate (the stream is far beyond the GPU's
+    capacity), then at half the sustained rate measured there (below
+    capacity), then the plain FP64 one-request-at-a-time path at that same
+    rate. Requests draw from a pool of matrices of the three generators."""
     import krans_b200 as kb
-    from krans_b200.serving import SolveRequest, solve_batch
     ctx = kb.Context(0)
-    pool = serving_pool(args.pool, args.nnz_lo, args.nnz_hi)
-    mats = [kb.CudaCsrMatrixAdapter.from_scipy(ctx, inst.A, fp32=True) for inst in pool]
-    # capacity of the batched mixed form on this pool (one launch over it)
-    reqs = [SolveRequest(M, kb.CyclicLanczosOptions(k=i.k, tol_abs=1e-12 * lower_norm_bound(i.A), tol_rel=0.0,
-                                                    cg_maxit=1000, precision=kb.Precision.MIXED), seed=j + 1)
-            for j, (i, M) in enumerate(zip(pool, mats))]
-    solve_batch(ctx, reqs)
-    ms = solve_batch(ctx, reqs)
-    cap = len(reqs) / (ms / 1e3)
-    low, clk_low = _clocked(lambda: _stream(ctx, pool, mats, 0.5 * cap, args.seconds, 1, 4, 1024, 11))
-    high, clk_high = _clocked(lambda: _stream(ctx, pool, mats, 4.0 * cap, args.seconds, 1, 4, 1024, 12))
-    base = _stream(ctx, pool, mats, 0.5 * cap, args.seconds, 0, 1, 1, 11)
+    t_gen = time.perf_counter()
+    pool = serving_pool(args.pool, args.nnz_lo, args.nnz_hi, args.kmax)
+    t_gen = time.perf_counter() - t_gen
+    mats = [kb.CudaCsrMatrixAdapter.from_scipy(ctx, inst.A, fp32=(solver == "cyclic")) for inst, solver in pool]
+    bounds = [1e-12 * lower_norm_bound(inst.A) for inst, _ in pool]
+    budget = 150 * 10**9
+    high, clk_high = _clocked(lambda: _stream(ctx, pool, mats, bounds, args.rate, args.seconds, 1, 4, 1024, 11, budget))
+    low_rate = max(0.05, 0.5 * high["sustained_solves_per_s"])
+    low, clk_low = _clocked(lambda: _stream(ctx, pool, mats, bounds, low_rate, args.seconds, 1, 4, 1024, 12, budget))
+    base = _stream(ctx, pool, mats, bounds, low_rate, args.seconds, 0, 1, 1, 12, budget)
+    nnz = [inst.A.nnz for inst, _ in pool]
     line = {
         "metric": "serving stream: sustained null-space solves/s and p50/p99 latency incl. queueing",
         "value": high["sustained_solves_per_s"], "unit": "solves/s", "higher_is_better": True, "n_gpus": 1,
-        "steps": 1, "warmup": 1, "ms_per_step": 1e3 * args.seconds, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32 SpMV/Krylov + f64 reorth/tiny-SVD/CG polish", "data": "synthetic",
-        "config": {"workload": f"Poisson arrivals over a pool of {args.pool} matrices (shift, incidence deg 6/8, "
-                               f"planted k<=8), nnz log-uniform [{args.nnz_lo:.0e}, {args.nnz_hi:.0e}]",
-                   "seconds_per_phase": args.seconds, "hbm_budget_gb": 150,
-                   "batched_capacity_solves_per_s": cap},
-        "below_capacity": dict(low, offered_rate=0.5 * cap, clocks=clk_low),
-        "oversubscribed": dict(high, offered_rate=4.0 * cap),
-        "plain_fp64_one_at_a_time": dict(base, offered_rate=0.5 * cap),
+        "steps": 1, "warmup": 0, "ms_per_step": 1e3 * args.seconds, "scaling": "weak", "vs_baseline": None,
+        "dtype": "cyclic: f32 SpMV/Krylov + f64 reorth/tiny-SVD/CG polish; LOBPCG: f64", "data": "synthetic",
+        "config": {"workload": f"Poisson arrivals at {args.rate:g}/s over {args.seconds:g} s; requests drawn from a "
+                               f"pool of {args.pool} matrices: graph incidence (deg 8, LOBPCG), planted kernel "
+                               f"(cyclic) and the batched workload's shift/incidence (cyclic), nnz log-uniform "
+                               f"[{args.nnz_lo:.0e}, {args.nnz_hi:.0e}], k in 1..{args.kmax}",
+                   "hbm_budget_gb": 150, "pool_nnz_total": int(sum(nnz)), "pool_nnz_max": int(max(nnz)),
+                   "pool_generation_s": t_gen,
+                   "accept": "||Au|| <= 1e-12 * max(row, col norm) (tol_abs, tol_rel = 0)"},
+        "oversubscribed": dict(high, clocks=clk_high),
+        "below_capacity": dict(low, clocks=clk_low),
+        "plain_fp64_one_at_a_time": dict(base, definition="FP64 cyclic requests and LOBPCG, one request per launch, "
+                                                          "one launch at a time, same arrivals as below_capacity"),
         "clocks": clk_high, "gpu_launches": None,
+        "tuning": {"table": ctx.tuning_table or "built-in defaults"},
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -930,10 +963,12 @@ def main():
     ap.add_argument("--max-restarts", type=int, default=400)
     ap.add_argument("--cg-maxit", type=int, default=1000, help="planted: CG iteration cap of the projector")
     ap.add_argument("--stagnation", type=int, default=30, help="planted: restarts without progress before stopping")
-    ap.add_argument("--pool", type=int, default=64)
+    ap.add_argument("--pool", type=int, default=36, help="serving: request matrices in the pool")
     ap.add_argument("--nnz-lo", type=float, default=1e4)
-    ap.add_argument("--nnz-hi", type=float, default=2e6)
-    ap.add_argument("--seconds", type=float, default=20.0)
+    ap.add_argument("--nnz-hi", type=float, default=5e7)
+    ap.add_argument("--kmax", type=int, default=64)
+    ap.add_argument("--rate", type=float, default=2000.0, help="serving: offered requests/s")
+    ap.add_argument("--seconds", type=float, default=60.0)
     args = ap.parse_args()
     if args.warmup < 3:
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)

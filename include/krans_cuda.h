@@ -340,7 +340,9 @@ typedef struct krans_request {
   krans_cyclic_opts opts;    /* options of a cyclic request (k, tolerances, precision) */
   uint32_t seed;             /* RNG seed of the request's own stream */
   int32_t rng_mode;          /* KRANS_RNG_PHILOX or KRANS_RNG_MT19937 */
-  double *basis_out;         /* DEVICE pointer: basis_capacity x cols(A) doubles, row i = vector i */
+  double *basis_out;         /* DEVICE pointer: basis_capacity x cols(A) doubles, row i = vector i;
+                                NULL: the basis stays in the request's workspace and is dropped
+                                (the result, max_residual included, is still reported) */
   int64_t basis_capacity;    /* vectors that fit in basis_out */
   int32_t solver;            /* KRANS_SOLVER_CYCLIC; KRANS_SOLVER_LOBPCG for krans_submit only */
   int32_t reserved;
@@ -419,7 +421,14 @@ int krans_server_destroy(krans_server *s);
 int krans_submit(krans_server *s, const krans_request *req, uint64_t *ticket);
 /* status: 0 queued, 1 running, 2 done, 3 failed, 4 cancelled */
 int krans_poll(krans_server *s, uint64_t ticket, int *status, krans_request_result *result);
+/* A queued request is dropped at once. A running one is stopped: the server
+ * writes KRANS_ERR_CANCELLED into its device status word, its team unwinds at
+ * its next check (every solver loop checks it), and the ticket ends as
+ * cancelled (status 4), or as done if it finished first. */
 int krans_cancel(krans_server *s, uint64_t ticket);
+/* Tickets finished (done, failed or cancelled) since the last call, oldest
+ * first, at most `capacity` of them; *count = how many were written. */
+int krans_server_completed(krans_server *s, uint64_t *tickets, int64_t capacity, int64_t *count);
 /* Block until every submitted request has finished or timeout_ms passes. */
 int krans_server_drain(krans_server *s, double timeout_ms);
 

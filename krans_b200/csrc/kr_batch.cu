@@ -143,8 +143,8 @@ struct BatchLaunch {
     KR_CHECK_ARG(r.opts.precond_aat >= KRANS_PRECOND_NONE && r.opts.precond_aat <= KRANS_PRECOND_SD &&
                      r.opts.precond_steps >= 1 && r.opts.precond_steps <= 1000,
                  "krans_solve_batch: precond_aat must be a KRANS_PRECOND_* value, precond_steps in [1, 1000]");
-    if (!trivial)
-      KR_CHECK_ARG(r.basis_out && r.basis_capacity >= kt, "krans_solve_batch: basis_out too small");
+    if (!trivial && r.basis_out)
+      KR_CHECK_ARG(r.basis_capacity >= kt, "krans_solve_batch: basis_out too small");
     q.trivial = trivial;
     q.plan.m = A->m;
     q.plan.n = A->n;
@@ -156,7 +156,7 @@ struct BatchLaunch {
     q.plan.cap = ncv / 2 + 2;
     q.plan.ksz = precision == KRANS_PREC_MIXED ? 4 : 8;
     q.plan.grid_blocks = 1;
-    q.plan.own_basis = 0;
+    q.plan.own_basis = r.basis_out ? 0 : 1; // no output buffer: the basis stays in the workspace
     q.plan.block_polish = r.opts.polish_block ? 1 : 0;
     q.plan.precond = r.opts.precond_aat;
     q.basis = r.basis_out;
@@ -180,6 +180,7 @@ struct BatchLaunch {
     p.cap = p.ncv / 2 + 2;
     p.ksz = precision == KRANS_PREC_MIXED ? 4 : 8;
     p.grid_blocks = 1;
+    p.own_basis = 1;
     return cyclic_carve(p, nullptr, nullptr);
   }
 
@@ -490,6 +491,14 @@ struct BatchLaunch {
     return 1;
   }
 
+  // stop a published request: its team sees the status word at its next
+  // check and unwinds (copied on `ctl`, beside the running kernel)
+  int cancel_slot(int g, cudaStream_t ctl) const {
+    static const int32_t cancelled = KRANS_ERR_CANCELLED;
+    cudaError_t e = cudaMemcpyAsync(d_status + g, &cancelled, 4, cudaMemcpyHostToDevice, ctl);
+    return e == cudaSuccess ? KRANS_OK : cuda_fail(e, "cancel request", __FILE__, __LINE__);
+  }
+
   void close() {
     if (open && feed) {
       std::atomic_thread_fence(std::memory_order_seq_cst);
@@ -642,6 +651,7 @@ int lobpcg_async_launch(LobpcgAsync *a, cudaStream_t s);
 bool lobpcg_async_done(const LobpcgAsync *a);
 void lobpcg_async_finish(const LobpcgAsync *a, krans_request_result *out);
 void lobpcg_async_release(LobpcgAsync *a);
+int lobpcg_async_cancel(LobpcgAsync *a, cudaStream_t ctl);
 } // namespace kr
 
 // a published large or mid request that no cluster claims for this long
@@ -681,8 +691,10 @@ struct krans_server {
   std::vector<cudaStream_t> streams;
   std::vector<bool> stream_busy;
   cudaEvent_t ctx_ready = nullptr; // orders launches after work queued on the context's stream
+  cudaStream_t ctl = nullptr;      // cancellations of running requests
   std::vector<InFlight *> inflight;
   InFlight *open = nullptr; // the launch that takes new cyclic requests
+  std::deque<uint64_t> completed; // finished tickets not yet handed out by krans_server_completed
   size_t bytes_in_use = 0;
   uint64_t next_ticket = 1;
   int64_t next_launch = 1;
@@ -696,19 +708,23 @@ struct krans_server {
         return (int)s;
     return -1;
   }
-  void fail(ServerTicket &t, int rc, Clock::time_point now) {
+  void fail(uint64_t id, int rc, Clock::time_point now) {
+    ServerTicket &t = tickets[id];
     memset(&t.res, 0, sizeof t.res);
     t.res.status = rc;
     t.state = 3;
     t.start_t = t.done_t = now;
     t.res.latency_ms = ms_since(t.submit_t, now);
+    completed.push_back(id);
   }
-  void finish(ServerTicket &t, Clock::time_point now, int64_t launch) {
+  void finish(uint64_t id, Clock::time_point now, int64_t launch) {
+    ServerTicket &t = tickets[id];
     t.done_t = now;
     t.res.queue_ms = ms_since(t.submit_t, t.start_t);
     t.res.latency_ms = ms_since(t.submit_t, now);
     t.res.launch_id = launch;
-    t.state = t.res.status == KRANS_OK ? 2 : 3;
+    t.state = t.res.status == KRANS_OK ? 2 : t.res.status == KRANS_ERR_CANCELLED ? 4 : 3;
+    completed.push_back(id);
   }
   bool admit_lobpcg(uint64_t id, Clock::time_point now);
   bool admit_cyclic(Clock::time_point now);
@@ -722,13 +738,13 @@ bool krans_server::admit_lobpcg(uint64_t id, Clock::time_point now) {
   size_t need = 0;
   int rc = lobpcg_async_plan(ctx, t.req, &a, &need);
   if (rc != KRANS_OK) {
-    fail(t, rc, now);
+    fail(id, rc, now);
     queue.pop_front();
     return true;
   }
   if (need > opts.hbm_budget_bytes) {
     lobpcg_async_release(a);
-    fail(t, KRANS_ERR_OUT_OF_MEMORY, now);
+    fail(id, KRANS_ERR_OUT_OF_MEMORY, now);
     queue.pop_front();
     return true;
   }
@@ -744,7 +760,7 @@ bool krans_server::admit_lobpcg(uint64_t id, Clock::time_point now) {
   queue.pop_front();
   if (rc != KRANS_OK) {
     lobpcg_async_release(a);
-    fail(t, rc, now);
+    fail(id, rc, now);
     return true;
   }
   auto *f = new InFlight();
@@ -783,7 +799,7 @@ bool krans_server::admit_cyclic(Clock::time_point now) {
     }
     if (r < 0) {
       queue.pop_front();
-      fail(head, r, now);
+      fail(id, r, now);
       return true;
     }
     open->L.close(); // it does not fit: let the open launch drain, start the next one
@@ -834,14 +850,14 @@ bool krans_server::admit_cyclic(Clock::time_point now) {
       }
   if (rc != KRANS_OK) {
     for (auto id2 : take)
-      fail(tickets[id2], rc, now);
+      fail(id2, rc, now);
     delete f;
     return true;
   }
   if (need > budget) {
     // a request larger than the whole budget can never be admitted
     for (auto id2 : take)
-      fail(tickets[id2], KRANS_ERR_OUT_OF_MEMORY, now);
+      fail(id2, KRANS_ERR_OUT_OF_MEMORY, now);
     delete f;
     return true;
   }
@@ -858,7 +874,7 @@ bool krans_server::admit_cyclic(Clock::time_point now) {
   rc = ew == cudaSuccess ? f->L.alloc_and_launch(streams[fs]) : cuda_fail(ew, "server stream order", __FILE__, __LINE__);
   if (rc != KRANS_OK) {
     for (auto id2 : take)
-      fail(tickets[id2], rc, now);
+      fail(id2, rc, now);
     f->L.release();
     delete f;
     return true;
@@ -892,9 +908,8 @@ void krans_server::run() {
       for (size_t i = 0; i < f->running.size();) {
         const auto &r = f->running[i];
         if (f->L.slot_done(r.slot)) {
-          ServerTicket &t = tickets[r.ticket];
-          f->L.fill_slot(r.slot, &t.res);
-          finish(t, now, f->id);
+          f->L.fill_slot(r.slot, &tickets[r.ticket].res);
+          finish(r.ticket, now, f->id);
           f->running.erase(f->running.begin() + (long)i);
           moved = true;
         } else {
@@ -916,21 +931,20 @@ void krans_server::run() {
         continue;
       }
       if (f->lob) {
-        ServerTicket &t = tickets[f->lob_ticket];
-        lobpcg_async_finish(f->lob, &t.res);
-        finish(t, now, f->id);
+        lobpcg_async_finish(f->lob, &tickets[f->lob_ticket].res);
+        finish(f->lob_ticket, now, f->id);
         lobpcg_async_release(f->lob);
       } else {
         for (auto it = f->running.rbegin(); it != f->running.rend(); ++it) {
           ServerTicket &t = tickets[it->ticket];
           if (f->L.slot_done(it->slot)) {
             f->L.fill_slot(it->slot, &t.res);
-            finish(t, now, f->id);
+            finish(it->ticket, now, f->id);
           } else if (!f->L.claimed(it->slot)) {
             t.state = 0; // published after its launch's teams had left: queue it again
             queue.push_front(it->ticket);
           } else {
-            fail(t, KRANS_ERR_RUNTIME, now);
+            fail(it->ticket, KRANS_ERR_RUNTIME, now);
           }
         }
         if (open == f)
@@ -1000,7 +1014,11 @@ int krans_server_create(krans_ctx *ctx, const krans_server_opts *opts, krans_ser
   }
   if (e == cudaSuccess)
     e = cudaEventCreateWithFlags(&s->ctx_ready, cudaEventDisableTiming);
+  if (e == cudaSuccess)
+    e = cudaStreamCreateWithFlags(&s->ctl, cudaStreamNonBlocking);
   if (e != cudaSuccess) {
+    if (s->ctl)
+      cudaStreamDestroy(s->ctl);
     for (auto st : s->streams)
       cudaStreamDestroy(st);
     if (s->ctx_ready)
@@ -1037,6 +1055,8 @@ int krans_server_destroy(krans_server *s) {
   }
   for (auto st : s->streams)
     cudaStreamDestroy(st);
+  if (s->ctl)
+    cudaStreamDestroy(s->ctl);
   if (s->ctx_ready)
     cudaEventDestroy(s->ctx_ready);
   delete s;
@@ -1083,18 +1103,43 @@ int krans_cancel(krans_server *s, uint64_t ticket) {
     set_error("krans_cancel: unknown ticket %llu", (unsigned long long)ticket);
     return KRANS_ERR_NOT_FOUND;
   }
+  if (it->second.state == 1) {
+    // running: write the cancellation into the request's device status word
+    for (InFlight *f : s->inflight) {
+      if (f->lob && f->lob_ticket == ticket)
+        return lobpcg_async_cancel(f->lob, s->ctl);
+      if (!f->lob)
+        for (const auto &r : f->running)
+          if (r.ticket == ticket)
+            return f->L.cancel_slot(r.slot, s->ctl);
+    }
+    return KRANS_OK; // it has just finished
+  }
   if (it->second.state != 0) {
-    set_error("krans_cancel: ticket %llu is no longer queued", (unsigned long long)ticket);
+    set_error("krans_cancel: ticket %llu has finished", (unsigned long long)ticket);
     return KRANS_ERR_RUNTIME;
   }
   it->second.state = 4;
   memset(&it->second.res, 0, sizeof it->second.res);
   it->second.res.status = KRANS_ERR_CANCELLED;
+  s->completed.push_back(ticket);
   for (auto q = s->queue.begin(); q != s->queue.end(); ++q)
     if (*q == ticket) {
       s->queue.erase(q);
       break;
     }
+  return KRANS_OK;
+}
+
+int krans_server_completed(krans_server *s, uint64_t *tickets, int64_t capacity, int64_t *count) {
+  KR_CHECK_ARG(s && count && (capacity == 0 || tickets), "krans_server_completed: NULL argument");
+  std::lock_guard<std::mutex> lk(s->mu);
+  int64_t k = 0;
+  while (k < capacity && !s->completed.empty()) {
+    tickets[k++] = s->completed.front();
+    s->completed.pop_front();
+  }
+  *count = k;
   return KRANS_OK;
 }
 

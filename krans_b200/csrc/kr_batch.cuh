@@ -105,7 +105,8 @@ __device__ __noinline__ void run_cta_request(TeamShared *sh, CyclicDesc *dp, con
     d.trans_run = rq.trans_run;
     d.rng = rq.rng;
     d.initial_right = rq.initial_right;
-    d.basis = rq.basis;
+    if (rq.basis) // else the basis stays in the workspace (own_basis)
+      d.basis = rq.basis;
     d.ldb = rq.plan.ldb;
     d.status = rq.status;
     d.res = rq.res;
@@ -203,7 +204,8 @@ __global__ void __launch_bounds__(512, KR_BATCH_MIN_BLOCKS)
       d.trans_run = rq.trans_run;
       d.rng = rq.rng;
       d.initial_right = rq.initial_right;
-      d.basis = rq.basis;
+      if (rq.basis) // else the basis stays in the workspace (own_basis)
+        d.basis = rq.basis;
       d.ldb = rq.plan.ldb;
       d.status = rq.status;
       d.res = rq.res;

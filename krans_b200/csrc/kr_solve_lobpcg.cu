@@ -391,7 +391,7 @@ int lobpcg_async_plan(krans_ctx *ctx, const krans_request &r, LobpcgAsync **out,
   }
   int64_t bs = o.block_size > 0 ? o.block_size : std::min<int64_t>(16, std::max<int64_t>(1, k_target));
   bs = std::min<int64_t>(bs, n);
-  if (bs > 128 || k_target > 512 || !r.basis_out || r.basis_capacity < k_target ||
+  if (bs > 128 || k_target > 512 || (r.basis_out && r.basis_capacity < k_target) ||
       o.precond_normal < KRANS_PRECOND_NONE || o.precond_normal > KRANS_PRECOND_SD || o.precond_steps < 1 ||
       o.precond_steps > 1000) {
     delete a;
@@ -474,7 +474,7 @@ int lobpcg_async_launch(LobpcgAsync *a, cudaStream_t s) {
     e = cudaMemcpyAsync(a->h_res, d.res, sizeof(LobpcgDevResult), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(a->h_mr, a->d_mr, sizeof(double), cudaMemcpyDeviceToHost, s);
-  if (e == cudaSuccess && a->k_target > 0)
+  if (e == cudaSuccess && a->k_target > 0 && a->req.basis_out)
     e = cudaMemcpy2DAsync(a->req.basis_out, (size_t)a->n * 8, d.RN, (size_t)d.ldn * 8, (size_t)a->n * 8,
                           (size_t)a->k_target, cudaMemcpyDeviceToDevice, s);
   if (e == cudaSuccess)
@@ -514,6 +514,14 @@ void lobpcg_async_finish(const LobpcgAsync *a, krans_request_result *out) {
   out->phase_ms[1] = R.phase_ms[1] + R.phase_ms[2];
   out->phase_ms[2] = R.phase_ms[3];
   out->phase_ms[3] = R.phase_ms[4];
+}
+
+int lobpcg_async_cancel(LobpcgAsync *a, cudaStream_t ctl) {
+  static const int32_t cancelled = KRANS_ERR_CANCELLED;
+  if (a->trivial || !a->ws)
+    return KRANS_OK;
+  cudaError_t e = cudaMemcpyAsync(a->d.status, &cancelled, 4, cudaMemcpyHostToDevice, ctl);
+  return e == cudaSuccess ? KRANS_OK : cuda_fail(e, "cancel request", __FILE__, __LINE__);
 }
 
 void lobpcg_async_release(LobpcgAsync *a) {

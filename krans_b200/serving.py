@@ -31,6 +31,7 @@ class SolveRequest:
     opts: object
     seed: int = 1
     rng_mode: str = "philox"
+    keep_basis: bool = True  # False: no output buffer; only the result (max_residual included)
     buf: Optional[CudaVectorAdapter] = None
     result: Optional[K.RequestResult] = None
     ticket: int = 0
@@ -51,7 +52,7 @@ class SolveRequest:
 
     def to_c(self, ctx: Context) -> K.Request:
         kt = max(self.k_target(), 1)
-        if self.buf is None:
+        if self.buf is None and self.keep_basis:
             self.buf = CudaVectorAdapter(ctx, kt * self.A.n)
         r = K.Request()
         r.A = self.A.h
@@ -64,14 +65,14 @@ class SolveRequest:
             r.opts = self.opts.to_c()
         r.seed = self.seed & 0xFFFFFFFF
         r.rng_mode = {"mt19937": K.KRANS_RNG_MT19937, "philox": K.KRANS_RNG_PHILOX}[self.rng_mode]
-        r.basis_out = self.buf.device_ptr()
-        r.basis_capacity = kt
+        r.basis_out = self.buf.device_ptr() if self.buf is not None else None
+        r.basis_capacity = kt if self.buf is not None else 0
         return r
 
     def basis(self) -> np.ndarray:
         """Accepted null vectors as rows (host copy)."""
         nr = int(self.result.n_right) if self.result is not None else 0
-        if nr == 0:
+        if nr == 0 or self.buf is None:
             return np.zeros((0, self.A.n))
         return self.buf.data()[: nr * self.A.n].reshape(nr, self.A.n)
 
@@ -121,7 +122,16 @@ class Server:
         return STATUS[st.value], res
 
     def cancel(self, ticket: int):
+        """Queued: dropped at once; running: stopped at its team's next status
+        check (the ticket ends as cancelled, or done if it finished first)."""
         check(self.ctx.lib.krans_cancel(self.h, ticket), "krans_cancel")
+
+    def completed(self, capacity: int = 4096):
+        """Tickets finished since the last call (krans_server_completed)."""
+        buf = (C.c_uint64 * capacity)()
+        n = C.c_int64()
+        check(self.ctx.lib.krans_server_completed(self.h, buf, capacity, C.byref(n)), "krans_server_completed")
+        return [int(buf[i]) for i in range(n.value)]
 
     def drain(self, timeout_s: float = 600.0):
         check(self.ctx.lib.krans_server_drain(self.h, timeout_s * 1e3), "krans_server_drain")

@@ -134,3 +134,36 @@ def test_lobpcg_request_errors(ctx):
     st, res = wait_done(srv, mixed.ticket)
     assert st == "failed" and res.status == -1  # LOBPCG requests run in FP64
     srv.close()
+
+
+def test_cancel_running_request_and_completed_list(ctx):
+    """A running request is stopped through its device status word (no wait
+    for it to finish); krans_server_completed hands out each finished ticket
+    once; a request without an output buffer still reports its residual."""
+    import krans_b200 as kb
+    from krans_b200.serving import Server, SolveRequest
+    d = G.difference_operator(200000)  # LOBPCG with block size 1 needs very many iterations here
+    M = kb.CudaCsrMatrixAdapter.from_scipy(ctx, d.A)
+    srv = Server(ctx, max_inflight=2)
+    slow = SolveRequest(M, kb.LOBPCGOptions(nev=1, block_size=1, max_iters=10**9), seed=3)
+    srv.submit(slow)
+    t0 = time.time()
+    while srv.poll(slow.ticket)[0] != "running" and time.time() - t0 < 60:
+        time.sleep(0.001)
+    time.sleep(0.2)
+    assert srv.poll(slow.ticket)[0] == "running"
+    t1 = time.time()
+    srv.cancel(slow.ticket)
+    st, res = wait_done(srv, slow.ticket, 60)
+    assert st == "cancelled" and res.status == -7 and time.time() - t1 < 30
+    inst = G.shift_operator(2000, 2, 0.5)
+    M2 = kb.CudaCsrMatrixAdapter.from_scipy(ctx, inst.A, fp32=True)
+    quick = cyclic_req(kb, ctx, inst, 5, [])
+    quick.keep_basis = False
+    srv.submit(quick)
+    st, res = wait_done(srv, quick.ticket)
+    assert st == "done" and res.converged_to_target and res.max_residual <= 1e-12 * norm_bound(inst.A)
+    assert quick.basis().shape == (0, inst.A.shape[1])
+    seen = srv.completed() + srv.completed()
+    assert sorted(seen) == sorted([slow.ticket, quick.ticket]) and srv.completed() == []
+    srv.close()
