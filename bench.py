@@ -661,9 +661,11 @@ def run_planted(args):
     A = inst.A
     L = lower_norm_bound(A)
     M = kb.CudaCsrMatrixAdapter.from_scipy(ctx, A, fp32=True)
+    precond = {"none": kb.Precond.NONE, "jacobi": kb.Precond.JACOBI, "sd": kb.Precond.SD}[args.precond]
     opt = kb.CyclicLanczosOptions(k=k, tol_abs=1e-12 * L, tol_rel=0.0, cg_maxit=args.cg_maxit, ncv=args.ncv,
                                   max_restarts=args.max_restarts, stagnation_restarts=args.stagnation,
-                                  precision=kb.Precision.MIXED)
+                                  precision=kb.Precision.MIXED, precond_aat=precond,
+                                  precond_steps=args.precond_steps)
 
     def solve():
         R = kb.find_nullspace_cyclic_lanczos_ex(M, kb.CudaVectorFactory(ctx, A.shape[1], seed=42, mode="philox"),
@@ -680,6 +682,7 @@ def run_planted(args):
         "data": "synthetic",
         "config": {"workload": f"planted kernel A=[B|BW], m={m}, n={A.shape[1]}, k={k}", "nnz": A.nnz,
                    "ncv": args.ncv, "max_restarts": args.max_restarts, "stagnation_restarts": args.stagnation,
+                   "precond_aat": args.precond, "precond_steps": args.precond_steps,
                    "accept": f"tol_abs=1e-12*max(row,col norm), tol_rel=0, cg_maxit={args.cg_maxit}"},
         "found": U.shape[0], "converged": R.converged_to_target, "restarts": R.restarts,
         "cg_solves": R.cg_solves, "cg_maxit_hits": R.cg_maxit_hits, "max_rel_residual": worst,
@@ -963,6 +966,9 @@ def main():
     ap.add_argument("--max-restarts", type=int, default=400)
     ap.add_argument("--cg-maxit", type=int, default=1000, help="planted: CG iteration cap of the projector")
     ap.add_argument("--stagnation", type=int, default=30, help="planted: restarts without progress before stopping")
+    ap.add_argument("--precond", choices=["none", "jacobi", "sd"], default="none",
+                    help="planted: device preconditioner of the CG projector on A A^T")
+    ap.add_argument("--precond-steps", type=int, default=8)
     ap.add_argument("--pool", type=int, default=36, help="serving: request matrices in the pool")
     ap.add_argument("--nnz-lo", type=float, default=1e4)
     ap.add_argument("--nnz-hi", type=float, default=5e7)

@@ -157,7 +157,6 @@ def test_cancel_running_request_and_completed_list(ctx):
     st, res = wait_done(srv, slow.ticket, 60)
     assert st == "cancelled" and res.status == -7 and time.time() - t1 < 30
     inst = G.shift_operator(2000, 2, 0.5)
-    M2 = kb.CudaCsrMatrixAdapter.from_scipy(ctx, inst.A, fp32=True)
     quick = cyclic_req(kb, ctx, inst, 5, [])
     quick.keep_basis = False
     srv.submit(quick)
