@@ -786,6 +786,70 @@ def run_spmv(args):
     return 0
 
 
+def run_gram(args):
+    """The block solver's dense products on their own, at the large-LOBPCG
+    workload's shapes: n = 64 x 2^s rows (s = --scale, 16 = 4,194,304), the
+    Gram S = Z^T Z, G = Z^T (AZ) of a p = 96 and a p = 288 block (the X and the
+    [X W P] blocks of block size 96) and the combination Z Y of a 288-column
+    block with a 288 x 96 matrix, FP64 tensor cores. FLOP/s count 2 n p^2 per
+    Gram (S and G: 4 n p^2), as form_gram's dot products do; the kernels form
+    the upper tiles only."""
+    import torch
+    import krans_b200 as kb
+    ctx = kb.Context(0)
+    n = 64 << args.scale
+    ld = n
+    out = {}
+
+    def measure():
+        g = torch.Generator(device="cuda:0").manual_seed(3)
+        for p in (96, 288):
+            Z = torch.randn(p, ld, dtype=torch.float64, device="cuda:0", generator=g)
+            W = torch.randn(p, ld, dtype=torch.float64, device="cuda:0", generator=g)
+            S = torch.empty(p, p, dtype=torch.float64, device="cuda:0")
+            G = torch.empty_like(S)
+            torch.cuda.synchronize()
+            for _ in range(max(3, args.warmup)):
+                kb.block_gram(ctx, n, p, Z.data_ptr(), ld, S.data_ptr(), W.data_ptr(), G.data_ptr())
+            ms = [kb.block_gram(ctx, n, p, Z.data_ptr(), ld, S.data_ptr(), W.data_ptr(), G.data_ptr())
+                  for _ in range(max(1, args.steps))]
+            t = statistics.median(ms) / 1e3
+            out[f"gram_p{p}"] = {"n": n, "p": p, "ms": t * 1e3, "tflops": 4.0 * n * p * p / t / 1e12,
+                                 "hbm_gbs": 2 * 8.0 * n * p / t / 1e9}
+            del W, S, G
+            if p == 288:
+                Cm = torch.randn(96, 288, dtype=torch.float64, device="cuda:0", generator=g)
+                O = torch.empty(96, ld, dtype=torch.float64, device="cuda:0")
+                torch.cuda.synchronize()
+                for _ in range(max(3, args.warmup)):
+                    kb.block_combine(ctx, n, 288, 96, Z.data_ptr(), ld, Cm.data_ptr(), 288, O.data_ptr())
+                ms = [kb.block_combine(ctx, n, 288, 96, Z.data_ptr(), ld, Cm.data_ptr(), 288, O.data_ptr())
+                      for _ in range(max(1, args.steps))]
+                t = statistics.median(ms) / 1e3
+                out["combine_288x96"] = {"n": n, "zc": 288, "q": 96, "ms": t * 1e3,
+                                         "tflops": 2.0 * n * 288 * 96 / t / 1e12,
+                                         "hbm_gbs": 8.0 * n * (288 + 96) / t / 1e9}
+                del Cm, O
+            del Z
+            torch.cuda.empty_cache()
+    _, clocks = _clocked(measure)
+    peak_fp64 = 40.0  # B200 FP64 tensor-core datasheet figure (no measured FP64 peak is available)
+    v = out["gram_p288"]["tflops"]
+    line = {
+        "metric": "LOBPCG dense products: FP64 tensor-core TFLOP/s (Gram of the 288-column block)",
+        "value": v, "unit": "TFLOP/s", "higher_is_better": True, "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": out["gram_p288"]["ms"], "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (normal random blocks)",
+        "config": {"workload": f"tall-skinny Gram and combination at n = {n} (the large-LOBPCG workload's rows)",
+                   "l2": f"operands {2 * 8 * n * 288 / 1e9:.1f} GB, larger than L2"},
+        "roofline": {"bound": "tensor", "achieved": v, "peak": peak_fp64, "unit": "TFLOP/s", "frac": v / peak_fp64,
+                     "peak_kind": "datasheet (FP64 tensor)", "traffic": None},
+        "cases": out, "clocks": clocks, "gpu_launches": 3 * (max(3, args.warmup) + max(1, args.steps)),
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def serving_pool(P, nnz_lo, nnz_hi, kmax=64, seed=7):
     """Request matrices of the serving stream: each draws one of three
     generators in turn, nnz log-uniform in [nnz_lo, nnz_hi]:
@@ -849,6 +913,7 @@ def _stream(ctx, pool, mats, bounds, rate, seconds, precision, max_inflight, max
     srv = Server(ctx, hbm_budget=budget, max_inflight=max_inflight, max_batch=max_batch)
     pending = {}
     lat, lat_kind = [], {"cyclic": [], "lobpcg": []}
+    by_gen = {}  # generator -> [completed, met the bound, not converged, residual above the bound]
     done = ok = offered = 0
     t0 = time.perf_counter()
     nxt = rng.exponential(1.0 / rate)
@@ -870,6 +935,11 @@ def _stream(ctx, pool, mats, bounds, rate, seconds, precision, max_inflight, max
                 done += 1
                 good = st == "done" and res.converged_to_target and res.max_residual <= bounds[i]
                 ok += int(good)
+                g = by_gen.setdefault(f"{pool[i][0].name}/{solver}", [0, 0, 0, 0])
+                g[0] += 1
+                g[1] += int(good)
+                g[2] += int(not res.converged_to_target)
+                g[3] += int(res.n_right > 0 and res.max_residual > bounds[i])
                 lat.append(res.latency_ms)
                 lat_kind[solver].append(res.latency_ms)
         time.sleep(0.001)
@@ -886,7 +956,9 @@ def _stream(ctx, pool, mats, bounds, rate, seconds, precision, max_inflight, max
             "sustained_solves_per_s": done / elapsed,
             "p50_ms": percentile(lat, 50), "p99_ms": percentile(lat, 99),
             "p50_ms_cyclic": percentile(lat_kind["cyclic"], 50), "p50_ms_lobpcg": percentile(lat_kind["lobpcg"], 50),
-            "completed_lobpcg": len(lat_kind["lobpcg"]), "unfinished_cancelled": unfinished}
+            "completed_lobpcg": len(lat_kind["lobpcg"]), "unfinished_cancelled": unfinished,
+            "by_generator": {k: dict(zip(["completed", "met_1e-12", "not_converged", "residual_above_bound"], v))
+                             for k, v in sorted(by_gen.items())}}
 
 
 def run_serving(args):
@@ -956,7 +1028,7 @@ def main():
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["batched", "quickstart", "lobpcg", "planted", "serving", "spmv"],
+    ap.add_argument("--workload", choices=["batched", "quickstart", "lobpcg", "planted", "serving", "spmv", "gram"],
                     default="batched")
     ap.add_argument("--scale", type=int, default=16, help="lobpcg/planted: log2 size (16 = full)")
     ap.add_argument("--max-iters", type=int, default=1000)
@@ -984,7 +1056,7 @@ def main():
         return run_reference(args)
     if args.workload != "batched":
         return {"quickstart": run_quickstart, "lobpcg": run_lobpcg_incidence, "planted": run_planted,
-                "serving": run_serving, "spmv": run_spmv}[args.workload](args)
+                "serving": run_serving, "spmv": run_spmv, "gram": run_gram}[args.workload](args)
     return run_ours(args)
 
 

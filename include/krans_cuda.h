@@ -182,6 +182,23 @@ typedef struct krans_spmv_tuning {
 int krans_csr_set_spmv_tuning(krans_mat *A, int trans, const krans_spmv_tuning *t);
 int krans_csr_get_spmv_tuning(const krans_mat *A, int trans, krans_spmv_tuning *t);
 
+/* ---- the block solver's dense products on raw device arrays -----------------
+ * (no reference counterpart: the device code that LOBPCG runs inside its
+ * kernel, exposed for tests and benchmarks; FP64 tensor cores). Z, W are
+ * column-major n x p blocks with leading dimension ld >= n; results are
+ * column-major with leading dimension p (Gram) or ld (combine). Synchronous
+ * on the context's stream.
+ * krans_block_gram: S = Z^T Z and, when W is given, G = Z^T W, formed on the
+ *   upper triangle and mirrored as form_gram does (LOBPCGSolver.cpp:67-80);
+ *   W and G are both NULL or both given.
+ * krans_block_combine: out = Z C for C zc x q (leading dimension ldc), as
+ *   combine_columns (LOBPCGSolver.cpp:122-134).
+ * device_ms (may be NULL) receives the kernel's device time. */
+int krans_block_gram(krans_ctx *ctx, int64_t n, int64_t p, const double *Z, const double *W, int64_t ld,
+                     double *S, double *G, double *device_ms);
+int krans_block_combine(krans_ctx *ctx, int64_t n, int64_t zc, int64_t q, const double *Z, int64_t ld,
+                        const double *C, int64_t ldc, double *out, double *device_ms);
+
 /* ---- random vectors: VectorFactory::create_random_of_size ------------------
  * KRANS_RNG_MT19937 reproduces std::mt19937(seed) + std::normal_distribution
  * <double>(0,1) as used by StdVectorFactory/EigenVectorFactory

@@ -165,6 +165,8 @@ SIGNATURES = {
     "krans_vec_dot_noalloc": [P, P, I64, P, P],
     "krans_spmv": [P, I, P, P],
     "krans_spmv_ex": [P, I, I, P, P],
+    "krans_block_gram": [P, I64, I64, P, P, I64, P, P, C.POINTER(D)],
+    "krans_block_combine": [P, I64, I64, I64, P, I64, P, I64, P, C.POINTER(D)],
     "krans_csr_set_spmv_tuning": [P, I, C.POINTER(SpmvTuning)],
     "krans_csr_get_spmv_tuning": [P, I, C.POINTER(SpmvTuning)],
     "krans_rng_create": [P, C.c_uint32, I, PP],

@@ -545,6 +545,22 @@ def read_matrix(path: str, fmt: int = K.KRANS_FMT_AUTO):
     return sp.csr_matrix((data, indices, indptr), shape=(M, N))
 
 
+def block_gram(ctx: Context, n: int, p: int, Z: int, ld: int, S: int, W: int = 0, G: int = 0) -> float:
+    """S = Z^T Z (and G = Z^T W) for column-major n x p device blocks given by
+    their addresses (krans_block_gram); returns the kernel's device ms."""
+    ms = C.c_double()
+    check(ctx.lib.krans_block_gram(ctx.h, n, p, Z, W or None, ld, S, G or None, C.byref(ms)), "krans_block_gram")
+    return ms.value
+
+
+def block_combine(ctx: Context, n: int, zc: int, q: int, Z: int, ld: int, Cm: int, ldc: int, out: int) -> float:
+    """out = Z C for a column-major n x zc device block and zc x q C
+    (krans_block_combine); returns the kernel's device ms."""
+    ms = C.c_double()
+    check(ctx.lib.krans_block_combine(ctx.h, n, zc, q, Z, ld, Cm, ldc, out, C.byref(ms)), "krans_block_combine")
+    return ms.value
+
+
 def basis_to_numpy(vs: Sequence[CudaVectorAdapter]) -> np.ndarray:
     if not vs:
         return np.zeros((0, 0))
