@@ -374,11 +374,68 @@ template <class Team> struct LobpcgSolver {
     return true;
   }
 
+  // The k columns of a block, KR_NBP at a time: Zi holds the group
+  // interleaved (row i's KR_NBP entries in 64 contiguous bytes), so the
+  // multi-right-hand-side SpMV (team_spmv_block) reads the operator once per
+  // group and every gather reads 64 contiguous bytes; each row is summed in
+  // storage order.
+  KR_DEV void interleave(const double *Zg, int gc) {
+    team_for(tm, n * KR_NBP, [&](int64_t e) {
+      const int64_t i = e / KR_NBP;
+      const int j = (int)(e % KR_NBP);
+      d.Zi[e] = j < gc ? Zg[(int64_t)j * ldn + i] : 0.0;
+    });
+    c.bytes += 16.0 * n * gc;
+    tm.sync();
+  }
+  // AZ = A^T (A Z) (LOBPCGSolver.cpp:54-64, column by column there): per
+  // group, Ti = A Zi, then the columns of A^T Ti straight into AZb
   __device__ __noinline__ void apply_normal(const double *Zb, int64_t k, double *AZb) {
     const uint64_t t0 = globaltimer_ns();
-    for (int64_t j = 0; j < k; j++) {
-      mulA(col((double *)Zb, j), d.tmv);
-      mulAT(d.tmv, col(AZb, j));
+    const int jc = (int)(tm.tid() % KR_NBP); // this thread's column within a group
+    for (int64_t g0 = 0; g0 < k; g0 += KR_NBP) {
+      const int gc = (int)imin64(KR_NBP, k - g0);
+      interleave(Zb + g0 * ldn, gc);
+      team_spmv_block(
+          tm, m, d.F.rp, d.F.ci, d.F.v64, d.F.ulen, jc < gc,
+          [&](int32_t cc) { return d.Zi[(int64_t)cc * KR_NBP + jc]; },
+          [&](int64_t i, double s) { d.Ti[i * KR_NBP + jc] = s; });
+      tm.sync();
+      double *out = AZb + (g0 + (jc < gc ? jc : 0)) * ldn;
+      team_spmv_block(
+          tm, n, d.B.rp, d.B.ci, d.B.v64, d.B.ulen, jc < gc,
+          [&](int32_t cc) { return d.Ti[(int64_t)cc * KR_NBP + jc]; }, [&](int64_t i, double s) { out[i] = s; });
+      tm.sync();
+      c.spmv += gc;
+      c.spmvT += gc;
+      c.bytes += gc * (spmv_bytes(m, n, d.F.nnz, 8, 8, 8) + spmv_bytes(n, m, d.B.nnz, 8, 8, 8));
+    }
+    t_ph[0] += globaltimer_ns() - t0;
+  }
+  // d.avn[j] = ||A x_j|| for the k columns of a block (the acceptance test's
+  // norms, LOBPCGSolver.cpp:545-560), through the same grouped SpMV; every
+  // block writes the team-wide totals and reads back only its own writes
+  __device__ __noinline__ void block_norms(const double *Xb, int64_t k) {
+    const uint64_t t0 = globaltimer_ns();
+    const int jc = (int)(tm.tid() % KR_NBP);
+    for (int64_t g0 = 0; g0 < k; g0 += KR_NBP) {
+      const int gc = (int)imin64(KR_NBP, k - g0);
+      interleave(Xb + g0 * ldn, gc);
+      double s2 = 0.0;
+      team_spmv_block(
+          tm, m, d.F.rp, d.F.ci, d.F.v64, d.F.ulen, jc < gc,
+          [&](int32_t cc) { return d.Zi[(int64_t)cc * KR_NBP + jc]; }, [&](int64_t, double s) { s2 += s * s; });
+      double v[KR_NBP];
+#pragma unroll
+      for (int j = 0; j < KR_NBP; j++)
+        v[j] = j == jc ? s2 : 0.0;
+      tm.template sum<KR_NBP>(v);
+      if (threadIdx.x == 0)
+        for (int j = 0; j < gc; j++)
+          d.avn[g0 + j] = sqrt(v[j]);
+      __syncthreads();
+      c.spmv += gc;
+      c.bytes += gc * spmv_bytes(m, n, d.F.nnz, 8, 8, 8);
     }
     t_ph[0] += globaltimer_ns() - t0;
   }
@@ -777,13 +834,22 @@ template <class Team> struct LobpcgSolver {
       ++its;
       int64_t nconv = 0;
       double best_unacc = INFINITY;
+      // residuals of all columns in one pass, R = AX - theta X, and the norms
+      // ||A x_j|| of the acceptance test for the whole block
+      {
+        for (int j = threadIdx.x; j < (int)bs; j += blockDim.x)
+          tm.sh->h[j] = theta_of(j);
+        __syncthreads();
+        const double *sth = tm.sh->h;
+        team_for(tm, bs * ldn, [&](int64_t e) { Rb[e] = AX[e] - sth[e / ldn] * X[e]; });
+        c.bytes += 24.0 * n * bs;
+        tm.sync();
+      }
+      block_norms(X, bs);
       for (int64_t j = 0; j < bs; ++j) {
         const double th = theta_of(j);
-        double *rj = col(Rb, j), *xj = col(X, j), *axj = col(AX, j);
-        team_for(tm, n, [&](int64_t i) { rj[i] = axj[i] - th * xj[i]; });
-        c.bytes += 24.0 * n;
-        tm.sync();
-        const double av_orig = normA(xj, d.tmv);
+        double *xj = col(X, j);
+        const double av_orig = *(volatile double *)&d.avn[j];
         if (av_orig <= accept_thr) {
           copy(xj, d.vacc);
           gs_pass(d.Yl, nlocked, d.vacc);

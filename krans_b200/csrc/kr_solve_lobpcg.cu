@@ -42,6 +42,9 @@ static size_t lobpcg_layout(int64_t m, int64_t n, int64_t bs, int64_t k, int64_t
   t.RN = c.take<double>(std::max<int64_t>(k, 1) * ldn);
   t.tmv = c.take<double>(ldm);
   t.vacc = c.take<double>(ldn);
+  t.Zi = c.take<double>(KR_NBP * ldn);
+  t.Ti = c.take<double>(KR_NBP * ldm);
+  t.avn = c.take<double>(bs);
   t.theta = c.take<double>(bs);
   t.th = c.take<double>(pmax);
   t.S = c.take<double>(pmax * pmax);

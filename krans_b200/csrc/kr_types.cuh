@@ -233,6 +233,7 @@ struct LobpcgDesc {
   double *X, *AX, *Rb, *W, *P, *T1, *T2, *Z, *AZ;
   double *Yl, *RN; // locked set and output basis (k_target columns)
   double *tmv, *vacc;
+  double *Zi, *Ti, *avn; // interleaved groups of KR_NBP columns (n and m rows), ||A x_j|| of the block
   double *theta, *th;
   // small dense matrices (pmax x pmax)
   double *S, *G, *Ym, *Sj, *Li, *Tm, *Cm, *Q;
