@@ -430,8 +430,10 @@ int krans_server_destroy(krans_server *s);
  * Cyclic requests join a running persistent launch when one has a free team
  * of their size class: the launch stays resident while requests keep
  * arriving (its teams leave after 20 ms without work) and leaves 20 SMs free
- * for other work; a request that does not fit it (another precision, a
- * larger workspace than its slots) starts the next launch. LOBPCG requests
+ * for other work; its thread-block clusters take large requests whenever
+ * one waits and single-block requests otherwise. A request that does not fit
+ * it (another precision, a larger workspace than its slots) starts the next
+ * launch. LOBPCG requests
  * run one per launch, on one thread block (m + n below the context's
  * cluster_min) or on a cluster of up to 4 blocks, FP64; their result reports
  * LOBPCG iterations in `restarts` and locked vectors in `krylov_steps_total`. */

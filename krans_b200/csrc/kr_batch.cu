@@ -109,11 +109,6 @@ struct BatchLaunch {
   std::vector<int64_t> slot_kt;                      // per slot: k_target
   cudaStream_t cs = nullptr;                         // publishing copies
   cudaEvent_t evc = nullptr;
-  int *h_qpoll = nullptr;                            // queue counters read while the launch runs
-  cudaEvent_t evq = nullptr;
-  bool qpoll_pending = false;
-  int last_count[3] = {0, 0, 0};                     // large / mid counters at their last advance
-  Clock::time_point last_advance[3];
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;
   std::vector<CyclicRequestDev> hreq;
   std::vector<RngState> hrng;
@@ -345,12 +340,6 @@ struct BatchLaunch {
       }
       if (e == cudaSuccess)
         e = cudaEventCreateWithFlags(&evc, cudaEventDisableTiming);
-      if (e == cudaSuccess)
-        e = cudaEventCreateWithFlags(&evq, cudaEventDisableTiming);
-      if (e == cudaSuccess)
-        e = cudaMallocHost(&h_qpoll, 4 * sizeof(int));
-      for (int q = 0; q < 3; q++)
-        last_advance[q] = Clock::now();
     }
     for (int pos = 0; pos < count; pos++) {
       const int g = slot_of(pos);
@@ -517,34 +506,6 @@ struct BatchLaunch {
     }
   }
 
-  // Open launch: true when queue q (0 large, 1 mid) has published requests
-  // that no team claimed and its counter has not moved for `stall_ms` (its
-  // clusters have turned to small requests, or are all held by long ones).
-  // The counters are read with an asynchronous copy on `ctl` (beside the
-  // running kernel); a call starts or collects one read.
-  bool stalled(int q, double stall_ms, cudaStream_t ctl) {
-    if (!open || npub[q] == 0)
-      return false;
-    const auto now = Clock::now();
-    if (!qpoll_pending) {
-      if (cudaMemcpyAsync(h_qpoll, d_queue, 4 * sizeof(int), cudaMemcpyDeviceToHost, ctl) == cudaSuccess &&
-          cudaEventRecord(evq, ctl) == cudaSuccess)
-        qpoll_pending = true;
-      return false;
-    }
-    if (cudaEventQuery(evq) != cudaSuccess)
-      return false;
-    qpoll_pending = false;
-    for (int k = 0; k < 2; k++) {
-      const int counter = h_qpoll[k == 0 ? 0 : 2];
-      if (counter > last_count[k]) {
-        last_count[k] = counter;
-        last_advance[k] = now;
-      }
-    }
-    return last_count[q] < npub[q] && ms_since(last_advance[q], now) > stall_ms;
-  }
-
   // queue of a slot, and whether a team claimed it (valid once done())
   int queue_of(int g) const { return g >= base[2] ? 2 : (g >= base[1] && cap[1] > 0) ? 1 : 0; }
   bool claimed(int g) const {
@@ -606,12 +567,6 @@ struct BatchLaunch {
       cudaFreeHost(h_mr);
     if (h_queue)
       cudaFreeHost(h_queue);
-    if (h_qpoll)
-      cudaFreeHost(h_qpoll);
-    h_qpoll = nullptr;
-    if (evq)
-      cudaEventDestroy(evq);
-    evq = nullptr;
     if (feed)
       cudaFreeHost(feed);
     if (hdone)
@@ -698,12 +653,6 @@ void lobpcg_async_finish(const LobpcgAsync *a, krans_request_result *out);
 void lobpcg_async_release(LobpcgAsync *a);
 int lobpcg_async_cancel(LobpcgAsync *a, cudaStream_t ctl);
 } // namespace kr
-
-// when the open launch's large (or mid) queue holds published requests and
-// its counter has not moved for this long (its clusters have turned to small
-// requests), the scheduler closes the launch so that it drains and the next
-// one takes them
-constexpr double kUnclaimedMs = 50.0;
 
 struct ServerTicket {
   krans_request req;
@@ -961,11 +910,6 @@ void krans_server::run() {
         } else {
           i++;
         }
-      }
-      // large or mid requests the open launch's clusters no longer take
-      if (f == open && !f->running.empty() && (f->L.stalled(0, kUnclaimedMs, ctl) || f->L.stalled(1, kUnclaimedMs, ctl))) {
-        f->L.close();
-        open = nullptr;
       }
     }
     // 2) launches that ended

@@ -32,7 +32,18 @@ extern __shared__ __align__(16) char kr_dyn_smem[];
 // published so far, claiming an index only once it is published; a team that
 // finds nothing sleeps between looks until the host publishes more, closes
 // the launch, or feed->idle_ns pass, and then leaves. Every wait is bounded.
-KR_DEV int take_request(int *queue, int count, const LaunchFeed *feed, int which) {
+// Open launches only: a published request of queue `which` that no team has
+// claimed yet.
+KR_DEV bool work_pending(const int *queue, const LaunchFeed *feed, int which) {
+  return *(volatile const int *)queue < *(volatile const int32_t *)&feed->published[which];
+}
+
+// In an open launch, -2 from take_request: no request of this queue, but the
+// `yield` queue has one waiting (the caller serves that queue first).
+constexpr int kTakeYield = -2;
+
+KR_DEV int take_request(int *queue, int count, const LaunchFeed *feed, int which, const int *yield_queue = nullptr,
+                        int yield_which = 0) {
   if (!feed) {
     const int it = atomicAdd(queue, 1);
     return it < count ? it : -1;
@@ -51,6 +62,8 @@ KR_DEV int take_request(int *queue, int count, const LaunchFeed *feed, int which
     }
     if (closed) // read before `published`: nothing more can come
       return -1;
+    if (yield_queue && work_pending(yield_queue, feed, yield_which))
+      return kTakeYield;
     if (globaltimer_ns() - t0 > feed->idle_ns)
       return -1;
     __nanosleep(nap);
@@ -170,6 +183,60 @@ __global__ void __launch_bounds__(512, KR_BATCH_MIN_BLOCKS) cyclic_batch_kernel(
 // every block of every cluster keeps going on its own with small requests
 // (one-block teams), so no SM idles while work of either kind remains.
 // Cluster c owns large slot c; block b owns small slot b.
+// One large request on this thread-block cluster, workspace in `slot`.
+template <class KT>
+__device__ __noinline__ void run_cluster_request(TeamShared *sh, CyclicDesc *dp, const CyclicRequestDev &rq,
+                                                 char *slot, unsigned rank, unsigned csize, int &cbuf) {
+  CyclicDesc &d = *dp;
+  if (threadIdx.x == 0) {
+    memset(&d, 0, sizeof d);
+    cyclic_carve(rq.plan, slot, &d);
+    d.F = rq.F;
+    d.B = rq.B;
+    d.o = rq.o;
+    d.k_target = rq.plan.k_target;
+    d.ncv = rq.plan.ncv;
+    d.trans_run = rq.trans_run;
+    d.rng = rq.rng;
+    d.initial_right = rq.initial_right;
+    if (rq.basis) // else the basis stays in the workspace (own_basis)
+      d.basis = rq.basis;
+    d.ldb = rq.plan.ldb;
+    d.status = rq.status;
+    d.res = rq.res;
+  }
+  __syncthreads();
+  if (rank == 0 && threadIdx.x == 0)
+    rq.res->t_begin = globaltimer_ns();
+  if (!rq.trivial) {
+    TeamCluster tm{sh, d.status, 0, cbuf, rank, csize};
+    CyclicSolver<TeamCluster, KT> s(tm, d);
+    s.run();
+    tm.sync();
+    const int64_t nf = *(volatile int64_t *)&d.res->n_found;
+    const double mr = team_max_residual(tm, d.F, d.basis, d.ldb, nf);
+    if (tm.leader())
+      *rq.max_resid = mr;
+    cbuf = tm.cbuf;
+  }
+  if (rank == 0 && threadIdx.x == 0) {
+    rq.res->t_end = globaltimer_ns();
+    publish_done(rq);
+  }
+  cooperative_groups::this_cluster().sync();
+}
+
+// Persistent kernel over a batch with large and small requests. Each
+// thread-block cluster takes large requests (a TeamCluster per request, the
+// cluster's rank 0 draws from the large queue); when there is none, every
+// block of every cluster goes on by itself with small requests (one-block
+// teams), so no SM idles while work of either kind remains. In a closed launch
+// (feed == nullptr) that happens once the large queue is empty. In an open
+// launch (the server publishes requests while it runs) the cluster serves
+// small requests while no large one is waiting and regroups as soon as one
+// is (each block checks before taking its next small request), and leaves
+// once neither queue has had work for the feed's idle time.
+// Cluster c owns large slot c; block b owns small slot b.
 template <class KT>
 __global__ void __launch_bounds__(512, KR_BATCH_MIN_BLOCKS)
     cyclic_batch_cluster_kernel(const CyclicRequestDev *reqs_large, int n_large, int *queue_large, char *ws_large,
@@ -179,69 +246,87 @@ __global__ void __launch_bounds__(512, KR_BATCH_MIN_BLOCKS)
   __shared__ TeamShared sh;
   __shared__ CyclicDesc d;
   __shared__ CyclicRequestDev rq;
-  __shared__ int s_item;
+  __shared__ int s_item, s_back;
   cooperative_groups::cluster_group cl = cooperative_groups::this_cluster();
   const unsigned rank = cl.block_rank(), csize = cl.num_blocks();
   char *slot = ws_large + (size_t)(blockIdx.x / csize) * stride_large;
-  int cbuf = 0;
-  for (;;) {
-    if (rank == 0 && threadIdx.x == 0)
-      s_item = take_request(queue_large, n_large, feed, feed_large);
-    cl.sync();
-    const int item = *cl.map_shared_rank(&s_item, 0);
-    cl.sync();
-    if (item < 0)
-      break;
-    load_request(&rq, reqs_large + item);
-    if (threadIdx.x == 0) {
-      memset(&d, 0, sizeof d);
-      cyclic_carve(rq.plan, slot, &d);
-      d.F = rq.F;
-      d.B = rq.B;
-      d.o = rq.o;
-      d.k_target = rq.plan.k_target;
-      d.ncv = rq.plan.ncv;
-      d.trans_run = rq.trans_run;
-      d.rng = rq.rng;
-      d.initial_right = rq.initial_right;
-      if (rq.basis) // else the basis stays in the workspace (own_basis)
-        d.basis = rq.basis;
-      d.ldb = rq.plan.ldb;
-      d.status = rq.status;
-      d.res = rq.res;
-    }
-    __syncthreads();
-    if (rank == 0 && threadIdx.x == 0)
-      rq.res->t_begin = globaltimer_ns();
-    if (!rq.trivial) {
-      TeamCluster tm{&sh, d.status, 0, cbuf, rank, csize};
-      CyclicSolver<TeamCluster, KT> s(tm, d);
-      s.run();
-      tm.sync();
-      const int64_t nf = *(volatile int64_t *)&d.res->n_found;
-      const double mr = team_max_residual(tm, d.F, d.basis, d.ldb, nf);
-      if (tm.leader())
-        *rq.max_resid = mr;
-      cbuf = tm.cbuf;
-    }
-    if (rank == 0 && threadIdx.x == 0) {
-      rq.res->t_end = globaltimer_ns();
-      publish_done(rq);
-    }
-    cl.sync();
-  }
-  // small requests, block by block (no cluster-wide synchronisation below)
   char *cslot = ws_small + (size_t)blockIdx.x * stride_small;
+  int cbuf = 0;
+  if (!feed) {
+    for (;;) {
+      if (rank == 0 && threadIdx.x == 0)
+        s_item = take_request(queue_large, n_large, nullptr, feed_large);
+      cl.sync();
+      const int item = *cl.map_shared_rank(&s_item, 0);
+      cl.sync();
+      if (item < 0)
+        break;
+      load_request(&rq, reqs_large + item);
+      run_cluster_request<KT>(&sh, &d, rq, slot, rank, csize, cbuf);
+    }
+    // small requests, block by block (no cluster-wide synchronisation below)
+    for (;;) {
+      if (threadIdx.x == 0)
+        s_item = take_request(queue_small, n_small, nullptr, 2);
+      __syncthreads();
+      const int item = s_item;
+      __syncthreads();
+      if (item < 0)
+        break;
+      load_request(&rq, reqs_small + item);
+      run_cta_request<KT>(&sh, &d, rq, cslot);
+    }
+    return;
+  }
   for (;;) {
+    // large requests while there are any; give way when only small ones wait
+    int large_end;
+    for (;;) {
+      if (rank == 0 && threadIdx.x == 0)
+        s_item = take_request(queue_large, n_large, feed, feed_large, queue_small, 2);
+      cl.sync();
+      const int item = *cl.map_shared_rank(&s_item, 0);
+      cl.sync();
+      if (item < 0) {
+        large_end = item;
+        break;
+      }
+      load_request(&rq, reqs_large + item);
+      run_cluster_request<KT>(&sh, &d, rq, slot, rank, csize, cbuf);
+    }
+    // small requests block by block, until large work waits (back to the
+    // cluster) or none comes for the idle time
     if (threadIdx.x == 0)
-      s_item = take_request(queue_small, n_small, feed, 2);
-    __syncthreads();
-    const int item = s_item;
-    __syncthreads();
-    if (item < 0)
+      s_back = 0;
+    for (;;) {
+      if (threadIdx.x == 0) {
+        // large work first; a block waiting for small work also returns when some arrives
+        int it = work_pending(queue_large, feed, feed_large)
+                     ? kTakeYield
+                     : take_request(queue_small, n_small, feed, 2, queue_large, feed_large);
+        if (it == kTakeYield) {
+          s_back = 1;
+          it = -1;
+        }
+        s_item = it;
+      }
+      __syncthreads();
+      const int item = s_item;
+      __syncthreads();
+      if (item < 0)
+        break;
+      load_request(&rq, reqs_small + item);
+      run_cta_request<KT>(&sh, &d, rq, cslot);
+    }
+    // regroup; leave when the large phase ended (not yielded) and no block
+    // came back for large work
+    cl.sync();
+    int back = 0;
+    for (unsigned r = 0; r < csize; r++)
+      back |= *cl.map_shared_rank(&s_back, r);
+    cl.sync();
+    if (!back && large_end != kTakeYield)
       break;
-    load_request(&rq, reqs_small + item);
-    run_cta_request<KT>(&sh, &d, rq, cslot);
   }
 }
 
