@@ -752,8 +752,8 @@ def run_spmv(args):
                 y = kb.CudaVectorAdapter(ctx, rows)
                 ref = (A.T @ x.data()) if trans else (A @ x.data())
                 for prec, w in ((K.KRANS_PREC_FP64, 8), (K.KRANS_PREC_MIXED, 4)):
-                    for kern in (K.KRANS_SPMV_AUTO, K.KRANS_SPMV_LANES):
-                        M.set_spmv_tuning(trans, kern)
+                    for kern, xl in ((K.KRANS_SPMV_AUTO, False), (K.KRANS_SPMV_AUTO, True), (K.KRANS_SPMV_LANES, False)):
+                        M.set_spmv_tuning(trans, kern, 0, x_evict_last=xl)
                         fn = (lambda: M.multiply_transpose(x, y, prec)) if trans else (lambda: M.multiply(x, y, prec))
                         for _ in range(max(3, args.warmup)):
                             fn()
@@ -761,7 +761,7 @@ def run_spmv(args):
                         err = float(np.max(np.abs(y.data() - ref)) / max(1e-300, np.max(np.abs(ref))))
                         gbs = spmv_bytes(rows, cols, A.nnz, w) / (ms * 1e-3) / 1e9
                         key = f"{name}_{'AT' if trans else 'A'}_{'f64' if w == 8 else 'f32'}_" \
-                              f"{'auto' if kern == K.KRANS_SPMV_AUTO else 'lanes'}"
+                              f"{'lanes' if kern == K.KRANS_SPMV_LANES else ('auto_xl' if xl else 'auto')}"
                         cases[key] = {"rows": rows, "cols": cols, "nnz": int(A.nnz), "us": ms * 1e3,
                                       "GBps": gbs, "frac": gbs / peak, "max_rel_err_vs_scipy": err}
                     M.set_spmv_tuning(trans, K.KRANS_SPMV_AUTO)

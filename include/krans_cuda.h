@@ -178,6 +178,8 @@ int krans_spmv_ex(const krans_mat *A, int trans, int precision, const krans_vec 
 typedef struct krans_spmv_tuning {
   int32_t kernel;         /* KRANS_SPMV_* */
   int32_t rows_per_block; /* ROWTILE: rows per block, 1..2048 (0 = automatic) */
+  int32_t x_evict_last;   /* UNIFORM / ROWTILE: gather x with the L2 evict-last policy (0 = normal) */
+  int32_t reserved;
 } krans_spmv_tuning;
 int krans_csr_set_spmv_tuning(krans_mat *A, int trans, const krans_spmv_tuning *t);
 int krans_csr_get_spmv_tuning(const krans_mat *A, int trans, krans_spmv_tuning *t);

@@ -50,7 +50,8 @@ class KransInvalidArgument(KransError, ValueError):
 
 
 class SpmvTuning(C.Structure):
-    _fields_ = [("kernel", C.c_int32), ("rows_per_block", C.c_int32)]
+    _fields_ = [("kernel", C.c_int32), ("rows_per_block", C.c_int32), ("x_evict_last", C.c_int32),
+                ("reserved", C.c_int32)]
 
 
 class BatchTuning(C.Structure):

@@ -250,11 +250,13 @@ class CudaCsrMatrixAdapter:
         self._chk(x, y, self.m, self.n, "multiply_transpose")
         check(self.ctx.lib.krans_spmv_ex(self.h, 1, precision, x.h, y.h), "multiply_transpose")
 
-    def set_spmv_tuning(self, trans: bool, kernel: int = K.KRANS_SPMV_AUTO, rows_per_block: int = 0):
+    def set_spmv_tuning(self, trans: bool, kernel: int = K.KRANS_SPMV_AUTO, rows_per_block: int = 0,
+                        x_evict_last: bool = False):
         """Kernel of multiply (trans False) / multiply_transpose (trans True):
         KRANS_SPMV_AUTO, _ROWTILE (rows_per_block rows per block, 0 = from the
-        mean row length), _UNIFORM (rows of 1, 2 or 4 entries) or _LANES."""
-        t = K.SpmvTuning(kernel, rows_per_block)
+        mean row length), _UNIFORM (rows of 1, 2 or 4 entries) or _LANES;
+        x_evict_last: gather x with the L2 evict-last policy."""
+        t = K.SpmvTuning(kernel, rows_per_block, int(bool(x_evict_last)), 0)
         check(self.ctx.lib.krans_csr_set_spmv_tuning(self.h, int(bool(trans)), C.byref(t)), "set_spmv_tuning")
 
     def spmv_tuning(self, trans: bool):

@@ -744,6 +744,7 @@ int krans_csr_set_spmv_tuning(krans_mat *A, int trans, const krans_spmv_tuning *
                "krans_csr_set_spmv_tuning: unknown kernel");
   KR_CHECK_ARG(t->rows_per_block >= 0 && t->rows_per_block <= 2048,
                "krans_csr_set_spmv_tuning: rows_per_block outside 0..2048");
+  KR_CHECK_ARG(t->x_evict_last == 0 || t->x_evict_last == 1, "krans_csr_set_spmv_tuning: x_evict_last must be 0 or 1");
   const int32_t ulen = trans ? A->ulenT : A->ulen;
   KR_CHECK_ARG(t->kernel != KRANS_SPMV_UNIFORM || ulen == 1 || ulen == 2 || ulen == 4,
                "krans_csr_set_spmv_tuning: UNIFORM needs every row to hold exactly 1, 2 or 4 entries");

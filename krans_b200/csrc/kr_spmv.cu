@@ -74,6 +74,22 @@ KR_DEV void ld_stream_pair(const float *a, uint64_t pol, float &x, float &y) {
                : "l"(a), "l"(pol));
 }
 
+KR_DEV uint64_t l2_evict_last_policy() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+// gather of x: read-only path, with the evict-last L2 policy when XL
+template <bool XL> KR_DEV double ld_x(const double *a, uint64_t pol) {
+  if constexpr (XL) {
+    double v;
+    asm volatile("ld.global.nc.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(a), "l"(pol));
+    return v;
+  } else {
+    return __ldg(a);
+  }
+}
+
 // round-to-nearest product and sum in the accumulation type (never fused)
 KR_DEV double mul_rn(double a, double b) { return __dmul_rn(a, b); }
 KR_DEV float mul_rn(float a, float b) { return __fmul_rn(a, b); }
@@ -84,7 +100,7 @@ constexpr int kSpmvThreads = 256;
 constexpr int kTileNnz = 2048; // entries staged per tile (8 per thread)
 
 // ---- uniform rows ----------------------------------------------------------
-template <int L, class VT>
+template <int L, class VT, bool XL>
 __global__ void __launch_bounds__(kSpmvThreads) spmv_uniform_kernel(int64_t rows, const int32_t *__restrict__ ci,
                                                                     const VT *__restrict__ val,
                                                                     const double *__restrict__ x,
@@ -92,6 +108,7 @@ __global__ void __launch_bounds__(kSpmvThreads) spmv_uniform_kernel(int64_t rows
   using Acc = VT; // FP64 values: FP64 sums; FP32 values: FP32 sums
   constexpr int R = 4; // rows in flight per thread
   const uint64_t pol = l2_evict_first_policy();
+  const uint64_t xpol = XL ? l2_evict_last_policy() : 0;
   const int64_t nt = (int64_t)gridDim.x * blockDim.x;
   for (int64_t i0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i0 < rows; i0 += R * nt) {
     int32_t c[R][L];
@@ -130,7 +147,7 @@ __global__ void __launch_bounds__(kSpmvThreads) spmv_uniform_kernel(int64_t rows
     for (int u = 0; u < R; u++)
 #pragma unroll
       for (int j = 0; j < L; j++)
-        xv[u][j] = (i0 + (int64_t)u * nt < rows) ? (Acc)__ldg(x + c[u][j]) : Acc(0);
+        xv[u][j] = (i0 + (int64_t)u * nt < rows) ? (Acc)ld_x<XL>(x + c[u][j], xpol) : Acc(0);
 #pragma unroll
     for (int u = 0; u < R; u++) {
       const int64_t i = i0 + (int64_t)u * nt;
@@ -147,7 +164,7 @@ __global__ void __launch_bounds__(kSpmvThreads) spmv_uniform_kernel(int64_t rows
 // ---- row tiles -------------------------------------------------------------
 // Block b owns rows [b*rb, b*rb + rb), rb <= RPT * 256; thread t owns the
 // block's rows t, t + 256, ... (at most RPT of them).
-template <int RPT, class VT>
+template <int RPT, class VT, bool XL>
 __global__ void __launch_bounds__(kSpmvThreads) spmv_rowtile_kernel(int64_t rows, int rb,
                                                                     const int32_t *__restrict__ rp,
                                                                     const int32_t *__restrict__ ci,
@@ -159,6 +176,7 @@ __global__ void __launch_bounds__(kSpmvThreads) spmv_rowtile_kernel(int64_t rows
   __shared__ Acc prod[kTileNnz];
   __shared__ int32_t srp[RPT * kSpmvThreads + 1];
   const uint64_t pol = l2_evict_first_policy();
+  const uint64_t xpol = XL ? l2_evict_last_policy() : 0;
   const int tid = threadIdx.x;
   for (int64_t blk = blockIdx.x; blk * rb < rows; blk += gridDim.x) {
     const int64_t r0 = blk * rb;
@@ -184,7 +202,7 @@ __global__ void __launch_bounds__(kSpmvThreads) spmv_rowtile_kernel(int64_t rows
       Acc xv[NPT];
 #pragma unroll
       for (int j = 0; j < NPT; j++)
-        xv[j] = (j * kSpmvThreads + tid < tn) ? (Acc)__ldg(x + c[j]) : Acc(0);
+        xv[j] = (j * kSpmvThreads + tid < tn) ? (Acc)ld_x<XL>(x + c[j], xpol) : Acc(0);
 #pragma unroll
       for (int j = 0; j < NPT; j++) {
         const int q = j * kSpmvThreads + tid;
@@ -244,7 +262,7 @@ int spmv_rows_per_block(int64_t rows, int64_t nnz) {
   return (int)rb;
 }
 
-template <class VT>
+template <class VT, bool XL>
 static cudaError_t spmv_launch_t(const SpmvOperand &A, const VT *val, const double *x, double *y, int sms,
                                  cudaStream_t s) {
   if (A.rows <= 0)
@@ -259,11 +277,11 @@ static cudaError_t spmv_launch_t(const SpmvOperand &A, const VT *val, const doub
     const int64_t want = (A.rows + 4 * kSpmvThreads - 1) / (4 * kSpmvThreads);
     const int g = (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)sms * 8));
     if (A.ulen == 1)
-      spmv_uniform_kernel<1, VT><<<g, kSpmvThreads, 0, s>>>(A.rows, A.ci, val, x, y);
+      spmv_uniform_kernel<1, VT, XL><<<g, kSpmvThreads, 0, s>>>(A.rows, A.ci, val, x, y);
     else if (A.ulen == 2)
-      spmv_uniform_kernel<2, VT><<<g, kSpmvThreads, 0, s>>>(A.rows, A.ci, val, x, y);
+      spmv_uniform_kernel<2, VT, XL><<<g, kSpmvThreads, 0, s>>>(A.rows, A.ci, val, x, y);
     else
-      spmv_uniform_kernel<4, VT><<<g, kSpmvThreads, 0, s>>>(A.rows, A.ci, val, x, y);
+      spmv_uniform_kernel<4, VT, XL><<<g, kSpmvThreads, 0, s>>>(A.rows, A.ci, val, x, y);
     return cudaGetLastError();
   }
   if (kind == KRANS_SPMV_LANES) {
@@ -277,20 +295,21 @@ static cudaError_t spmv_launch_t(const SpmvOperand &A, const VT *val, const doub
   const int64_t nblk = (A.rows + rb - 1) / rb;
   const int g = (int)std::min<int64_t>(nblk, 1 << 30);
   if (rb <= kSpmvThreads)
-    spmv_rowtile_kernel<1, VT><<<g, kSpmvThreads, 0, s>>>(A.rows, rb, A.rp, A.ci, val, x, y);
+    spmv_rowtile_kernel<1, VT, XL><<<g, kSpmvThreads, 0, s>>>(A.rows, rb, A.rp, A.ci, val, x, y);
   else if (rb <= 2 * kSpmvThreads)
-    spmv_rowtile_kernel<2, VT><<<g, kSpmvThreads, 0, s>>>(A.rows, rb, A.rp, A.ci, val, x, y);
+    spmv_rowtile_kernel<2, VT, XL><<<g, kSpmvThreads, 0, s>>>(A.rows, rb, A.rp, A.ci, val, x, y);
   else if (rb <= 4 * kSpmvThreads)
-    spmv_rowtile_kernel<4, VT><<<g, kSpmvThreads, 0, s>>>(A.rows, rb, A.rp, A.ci, val, x, y);
+    spmv_rowtile_kernel<4, VT, XL><<<g, kSpmvThreads, 0, s>>>(A.rows, rb, A.rp, A.ci, val, x, y);
   else
-    spmv_rowtile_kernel<8, VT><<<g, kSpmvThreads, 0, s>>>(A.rows, rb, A.rp, A.ci, val, x, y);
+    spmv_rowtile_kernel<8, VT, XL><<<g, kSpmvThreads, 0, s>>>(A.rows, rb, A.rp, A.ci, val, x, y);
   return cudaGetLastError();
 }
 
 cudaError_t spmv_launch(const SpmvOperand &A, bool fp32, const double *x, double *y, int sms, cudaStream_t s) {
+  const bool xl = A.tune.x_evict_last != 0;
   if (fp32)
-    return spmv_launch_t<float>(A, A.v32, x, y, sms, s);
-  return spmv_launch_t<double>(A, A.v64, x, y, sms, s);
+    return xl ? spmv_launch_t<float, true>(A, A.v32, x, y, sms, s) : spmv_launch_t<float, false>(A, A.v32, x, y, sms, s);
+  return xl ? spmv_launch_t<double, true>(A, A.v64, x, y, sms, s) : spmv_launch_t<double, false>(A, A.v64, x, y, sms, s);
 }
 
 } // namespace kr

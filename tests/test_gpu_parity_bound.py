@@ -6,9 +6,10 @@ and the basis is within subspace distance 1e-10 (largest principal-angle sine
 the same options, and of the analytic kernel. Each device basis is also
 cross-checked with the reference's RREF subspace compare
 (include/krans/Utils/SubspaceCompare.hpp:86-110, restated in the oracle):
-the RREF forms of two bases of one subspace agree to 1e-8 (RREF divides by
-pivot entries, so it amplifies rounding; the principal-angle bound is the
-sharp one).
+the RREF forms of two bases of one subspace agree to 1e-8, or, where the
+subspace's RREF pivot block is ill-conditioned (RREF divides by it), to ten
+times the RREF gain measured on the reference basis itself times the
+principal-angle distance (the principal-angle bound is the sharp one).
 
 Solver options follow the accuracy target: tol_abs = 1e-12 L, tol_rel = 0.
 Where the reference algorithm itself cannot reach that target (the golden
@@ -33,16 +34,37 @@ def norm_bound(A):
     return float(np.sqrt(max(A2.sum(axis=0).max(), A2.sum(axis=1).max())))
 
 
+def rref_gain(oracle, ref):
+    """How much the RREF compare magnifies a principal-angle difference for
+    the subspace of `ref`: RREF divides by the basis entries at its pivot
+    columns, so the gain is the conditioning of that pivot block. Measured on
+    ref itself: the RREF difference to a rotated copy perturbed at 1e-12,
+    divided by that copy's subspace distance."""
+    rng = np.random.default_rng(0)
+    k, n = ref.shape
+    Q, _ = np.linalg.qr(rng.standard_normal((k, k)))
+    P = Q @ ref + 1e-12 * rng.standard_normal((k, n)) / np.sqrt(n)
+    P = np.linalg.qr(P.T)[0].T
+    return oracle.subspace_diff_rref(ref, P) / max(oracle.subspace_dist(ref, P), 1e-300)
+
+
+def rref_ok(oracle, ref, U, rref):
+    # the RREF forms agree to `rref`, or to what the RREF's own gain makes of
+    # the two bases' principal-angle distance (ill-conditioned pivot blocks)
+    d = oracle.subspace_diff_rref(ref, U)
+    return d <= max(rref, 10.0 * rref_gain(oracle, ref) * max(oracle.subspace_dist(ref, U), 1e-15))
+
+
 def check_basis(oracle, A, U, ref, kernel=None, dist=DIST, resid=RESID, rref=RREF):
     L = norm_bound(A)
     assert U.shape == ref.shape, (U.shape, ref.shape)
     assert max(np.linalg.norm(A @ u) for u in U) / L <= resid
     assert oracle.max_pairwise_abs_dot(U) <= 1e-12
     assert oracle.subspace_dist(ref, U) <= dist
-    assert oracle.subspace_diff_rref(ref, U) <= rref
+    assert rref_ok(oracle, ref, U, rref)
     if kernel is not None:
         assert oracle.subspace_dist(kernel, U) <= dist
-        assert oracle.subspace_diff_rref(kernel, U) <= rref
+        assert rref_ok(oracle, kernel, U, rref)
 
 
 def lobpcg_pair(ctx, oracle, A, seed, **kw):
@@ -93,7 +115,7 @@ def test_lobpcg_golden_default_tolerance_vs_oracle(ctx, oracle, k):
     assert max(np.linalg.norm(A @ u) for u in U) <= thr
     assert oracle.subspace_dist(O.right_null, U) <= 1e-8
     assert oracle.subspace_dist(dense_kernel(A, nul), U) <= 1e-8
-    assert oracle.subspace_diff_rref(O.right_null, U) <= 1e-6
+    assert rref_ok(oracle, O.right_null, U, 1e-6)
 
 
 @pytest.mark.parametrize("team", [1, 2])

@@ -90,6 +90,9 @@ def test_spmv_bit_identical_to_oracle(ctx, oracle, name):
             np.testing.assert_array_equal(y.data(), want64, err_msg=f"{name} trans={trans} kernel={kern} rb={rb}")
             mul(x, y, precision=kb.Precision.MIXED)
             np.testing.assert_array_equal(y.data(), want32, err_msg=f"f32 {name} trans={trans} kernel={kern}")
+        M.set_spmv_tuning(trans, K.KRANS_SPMV_AUTO, 0, x_evict_last=True)  # cache policy only
+        mul(x, y)
+        np.testing.assert_array_equal(y.data(), want64)
         M.set_spmv_tuning(trans, K.KRANS_SPMV_LANES)
         mul(x, y)
         bound = 64 * 2.2e-16 * (abs(Aop) @ np.abs(xh))
