@@ -227,6 +227,7 @@ def run_reference(args):
     run do not count against it."""
     import multiprocessing as mp
     rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
         return 0
     from oracle import oracle as O
@@ -252,7 +253,7 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": v, "unit": "solves/s",
         "higher_is_better": True, "n_gpus": 0, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * wall / max(1, args.steps), "dtype": "f64", "data": "synthetic",
-        "config": batched_config(args, 1),
+        "config": batched_config(args, world),
         "cpu_baseline": {"value": v, "unit": "solves/s", "cores": cores, "kind": kind,
                          "sample": f"{len(sample)} instances, one per timed step, stratified over the whole nnz "
                                    f"range of that step's {args.batch}-instance batch ({S} strata); rate = cores / "
