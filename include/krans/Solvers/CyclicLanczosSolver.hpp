@@ -53,6 +53,7 @@ struct CyclicLanczosOptions {
   int polish_block = 0; // 1: project up to 8 candidates per restart with one block CG
   int precond_device = KRANS_PRECOND_NONE; // device form of precond_AAt (KRANS_PRECOND_JACOBI / _SD)
   int precond_steps = 8;
+  bool mixed_fallback = true; // MIXED: continue in FP64 when the FP64 polish cannot finish FP32 Ritz vectors
 };
 
 struct CyclicLanczosResult {
@@ -103,6 +104,7 @@ inline CyclicLanczosResult find_nullspace_cyclic_lanczos_ex(const MatrixInterfac
   o.polish_block = opt.polish_block;
   o.precond_aat = opt.precond_device;
   o.precond_steps = opt.precond_steps;
+  o.mixed_fallback = opt.mixed_fallback ? 1 : 0;
   const krans_vec *y0 = nullptr;
   if (!opt.initial_right_space.empty() && opt.initial_right_space.front()) {
     const auto *c = dynamic_cast<const cuda::CudaVectorAdapter *>(opt.initial_right_space.front().get());

@@ -193,11 +193,16 @@ int krans_csr_get_spmv_tuning(const krans_mat *A, int trans, krans_spmv_tuning *
  * krans_block_gram: S = Z^T Z and, when W is given, G = Z^T W, formed on the
  *   upper triangle and mirrored as form_gram does (LOBPCGSolver.cpp:67-80);
  *   W and G are both NULL or both given.
+ * krans_block_gemm_tn: C = A^T B (a x b, leading dimension a) for n x a and
+ *   n x b blocks A, B (the projections onto the locked basis of
+ *   orthonormalize_block, LOBPCGSolver.cpp:137-160).
  * krans_block_combine: out = Z C for C zc x q (leading dimension ldc), as
  *   combine_columns (LOBPCGSolver.cpp:122-134).
  * device_ms (may be NULL) receives the kernel's device time. */
 int krans_block_gram(krans_ctx *ctx, int64_t n, int64_t p, const double *Z, const double *W, int64_t ld,
                      double *S, double *G, double *device_ms);
+int krans_block_gemm_tn(krans_ctx *ctx, int64_t n, int64_t a, const double *A, int64_t b, const double *B,
+                        int64_t ld, double *C, double *device_ms);
 int krans_block_combine(krans_ctx *ctx, int64_t n, int64_t zc, int64_t q, const double *Z, int64_t ld,
                         const double *C, int64_t ldc, double *out, double *device_ms);
 
@@ -271,6 +276,12 @@ typedef struct krans_cyclic_opts {
                                 0: polish candidates one by one (the reference's order);
                                 1: project up to 8 candidates of a restart with one block CG
                                 (matrix read once per iteration for all of them) */
+  int32_t mixed_fallback;    /* 1    KRANS_PREC_MIXED only: when the mixed run stops short of k
+                                with its FP64 CG polish at cg_maxit (FP32 Ritz vectors too far
+                                from the null space for the projector to finish), the solve
+                                continues in FP64 from the vectors already accepted (same RNG
+                                stream; krans_cyclic_result.fp64_fallback reports it). Single
+                                solves only: the batched and served paths keep the mixed result. */
 } krans_cyclic_opts;
 
 typedef struct krans_cyclic_result {
@@ -286,6 +297,8 @@ typedef struct krans_cyclic_result {
   double algo_bytes;         /* algorithmic HBM bytes of the solve */
   double device_ms;          /* device time of the solve kernel(s) */
   double phase_ms[4];        /* device time in Golub-Kahan+reorth, tiny SVD, CG polish, rest */
+  int32_t fp64_fallback;     /* 1 when a mixed solve continued in FP64 (mixed_fallback) */
+  int32_t fallback_from;     /* vectors the mixed run had accepted before it */
 } krans_cyclic_result;
 
 typedef struct krans_lobpcg_opts {

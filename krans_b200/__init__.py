@@ -9,7 +9,7 @@ from ._capi import KransError, KransInvalidArgument  # noqa: F401
 from .api import (  # noqa: F401
     Context, CudaCsrMatrixAdapter, CudaVectorAdapter, CudaVectorFactory,
     CyclicLanczosOptions, CyclicLanczosResult, LOBPCGOptions, LOBPCGResult,
-    Precision, Precond, ReorthMode, basis_to_numpy, block_combine, block_gram, default_context,
+    Precision, Precond, ReorthMode, basis_to_numpy, block_combine, block_gemm_tn, block_gram, default_context,
     find_nullspace_cyclic_lanczos, find_nullspace_cyclic_lanczos_ex,
     find_nullspace_lobpcg, find_nullspace_lobpcg_ex, read_matrix,
 )
@@ -18,7 +18,7 @@ __all__ = [
     "Context", "CudaCsrMatrixAdapter", "CudaVectorAdapter", "CudaVectorFactory",
     "CyclicLanczosOptions", "CyclicLanczosResult", "LOBPCGOptions", "LOBPCGResult",
     "Precision", "Precond", "ReorthMode", "KransError", "KransInvalidArgument", "basis_to_numpy",
-    "block_combine", "block_gram",
+    "block_combine", "block_gemm_tn", "block_gram",
     "default_context", "find_nullspace_cyclic_lanczos", "find_nullspace_cyclic_lanczos_ex",
     "find_nullspace_lobpcg", "find_nullspace_lobpcg_ex", "read_matrix",
 ]

@@ -69,7 +69,8 @@ class CyclicOpts(C.Structure):
                 ("frob_samples", C.c_int32), ("prescreen_factor", C.c_double),
                 ("stagnation_restarts", C.c_int64), ("return_left_space", C.c_int32),
                 ("verbose", C.c_int32), ("precision", C.c_int32), ("team", C.c_int32),
-                ("precond_aat", C.c_int32), ("precond_steps", C.c_int32), ("polish_block", C.c_int32)]
+                ("precond_aat", C.c_int32), ("precond_steps", C.c_int32), ("polish_block", C.c_int32),
+                ("mixed_fallback", C.c_int32)]
 
 
 class CyclicResultC(C.Structure):
@@ -78,7 +79,8 @@ class CyclicResultC(C.Structure):
                 ("converged_to_target", C.c_int32), ("status", C.c_int32),
                 ("cg_solves", C.c_int64), ("cg_maxit_hits", C.c_int64),
                 ("spmv", C.c_int64), ("spmvT", C.c_int64), ("algo_bytes", C.c_double),
-                ("device_ms", C.c_double), ("phase_ms", C.c_double * 4)]
+                ("device_ms", C.c_double), ("phase_ms", C.c_double * 4),
+                ("fp64_fallback", C.c_int32), ("fallback_from", C.c_int32)]
 
 
 class LobpcgOpts(C.Structure):
@@ -167,6 +169,7 @@ SIGNATURES = {
     "krans_spmv": [P, I, P, P],
     "krans_spmv_ex": [P, I, I, P, P],
     "krans_block_gram": [P, I64, I64, P, P, I64, P, P, C.POINTER(D)],
+    "krans_block_gemm_tn": [P, I64, I64, P, I64, P, I64, P, C.POINTER(D)],
     "krans_block_combine": [P, I64, I64, I64, P, I64, P, I64, P, C.POINTER(D)],
     "krans_csr_set_spmv_tuning": [P, I, C.POINTER(SpmvTuning)],
     "krans_csr_get_spmv_tuning": [P, I, C.POINTER(SpmvTuning)],

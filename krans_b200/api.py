@@ -368,6 +368,9 @@ class CyclicLanczosOptions:
     precond_aat: Precond = Precond.NONE  # device form of precond_AAt (Precond.JACOBI or Precond.SD)
     precond_steps: int = 8                   # steps of the SD preconditioner
     polish_block: int = 0  # 1: block CG polish of up to 8 candidates at once
+    # MIXED only: continue in FP64 when the mixed run stops short of k with its
+    # FP64 polish at cg_maxit (single solves; not the batched/served paths)
+    mixed_fallback: bool = True
 
     def to_c(self) -> K.CyclicOpts:
         o = K.CyclicOpts()
@@ -393,6 +396,8 @@ class CyclicLanczosResult:
     algo_bytes: float = 0.0
     device_ms: float = 0.0
     phase_ms: tuple = (0.0, 0.0, 0.0, 0.0)
+    fp64_fallback: bool = False  # the mixed solve continued in FP64
+    fallback_from: int = 0       # vectors the mixed run had accepted before that
 
 
 @dataclass
@@ -476,7 +481,8 @@ def find_nullspace_cyclic_lanczos_ex(A: CudaCsrMatrixAdapter, vf: CudaVectorFact
         frob_norm_est=res.frob_norm_est, converged_to_target=bool(res.converged_to_target),
         cg_solves=res.cg_solves, cg_maxit_hits=res.cg_maxit_hits, spmv=res.spmv,
         spmvT=res.spmvT, algo_bytes=res.algo_bytes, device_ms=res.device_ms,
-        phase_ms=tuple(res.phase_ms))
+        phase_ms=tuple(res.phase_ms), fp64_fallback=bool(res.fp64_fallback),
+        fallback_from=res.fallback_from)
     return R
 
 
@@ -552,6 +558,15 @@ def block_gram(ctx: Context, n: int, p: int, Z: int, ld: int, S: int, W: int = 0
     their addresses (krans_block_gram); returns the kernel's device ms."""
     ms = C.c_double()
     check(ctx.lib.krans_block_gram(ctx.h, n, p, Z, W or None, ld, S, G or None, C.byref(ms)), "krans_block_gram")
+    return ms.value
+
+
+def block_gemm_tn(ctx: Context, n: int, a: int, A: int, b: int, B: int, ld: int, Cm: int) -> float:
+    """C = A^T B (a x b, column-major) for column-major n x a and n x b device
+    blocks given by their addresses (krans_block_gemm_tn); returns the
+    kernel's device ms."""
+    ms = C.c_double()
+    check(ctx.lib.krans_block_gemm_tn(ctx.h, n, a, A, b, B, ld, Cm, C.byref(ms)), "krans_block_gemm_tn")
     return ms.value
 
 

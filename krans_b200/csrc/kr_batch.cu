@@ -302,12 +302,12 @@ struct BatchLaunch {
 
   int alloc_and_launch(cudaStream_t s) {
     stream = s;
-    int rc = dev_alloc(ctx, (void **)&ws, ws_bytes);
+    int rc = dev_alloc_async(ctx, (void **)&ws, ws_bytes, s);
     if (rc != KRANS_OK)
       return rc;
-    rc = dev_alloc(ctx, (void **)&meta, meta_bytes);
+    rc = dev_alloc_async(ctx, (void **)&meta, meta_bytes, s);
     if (rc != KRANS_OK) {
-      dev_free(ctx, ws, ws_bytes);
+      dev_free_async(ctx, ws, ws_bytes, s);
       ws = nullptr;
       return rc;
     }
@@ -388,6 +388,8 @@ struct BatchLaunch {
       e = cudaMemsetAsync(d_queue, 0, 4 * sizeof(int), s);
     if (e == cudaSuccess)
       e = cudaEventRecord(ev0, s);
+    if (e == cudaSuccess && cs) // publishing copies land in the stream-ordered allocation: after its set-up
+      e = cudaStreamWaitEvent(cs, ev0, 0);
     char *ws_small = ws, *ws_small_p = ws + (size_t)grid * ws_stride;
     char *ws_large = ws_small_p + (size_t)2 * npairs * ws_stride;
     char *ws_mid = ws_large + (size_t)nclusters * stride_L;
@@ -552,25 +554,24 @@ struct BatchLaunch {
     fill_result(r, h_mr[pos], h_status[pos], hreq[pos].trivial != 0, hreq[pos].plan.k_target, out);
   }
 
-  void release() {
+  // Device memory is freed in the launch's stream order (cudaFreeAsync: no
+  // wait for other launches still running); pinned host buffers go to
+  // `graveyard` when one is given (cudaFreeHost waits for the whole device;
+  // the server frees them once nothing runs), else are freed here.
+  void release(std::vector<void *> *graveyard = nullptr) {
     if (ws)
-      dev_free(ctx, ws, ws_bytes);
+      dev_free_async(ctx, ws, ws_bytes, stream);
     if (meta)
-      dev_free(ctx, meta, meta_bytes);
+      dev_free_async(ctx, meta, meta_bytes, stream);
     ws = meta = nullptr;
     d_reqs = nullptr;
-    if (h_res)
-      cudaFreeHost(h_res);
-    if (h_status)
-      cudaFreeHost(h_status);
-    if (h_mr)
-      cudaFreeHost(h_mr);
-    if (h_queue)
-      cudaFreeHost(h_queue);
-    if (feed)
-      cudaFreeHost(feed);
-    if (hdone)
-      cudaFreeHost(hdone);
+    for (void *h : {(void *)h_res, (void *)h_status, (void *)h_mr, (void *)h_queue, (void *)feed, (void *)hdone})
+      if (h) {
+        if (graveyard)
+          graveyard->push_back(h);
+        else
+          cudaFreeHost(h);
+      }
     h_res = nullptr;
     h_status = nullptr;
     h_mr = nullptr;
@@ -650,13 +651,14 @@ int lobpcg_async_plan(krans_ctx *ctx, const krans_request &r, LobpcgAsync **out,
 int lobpcg_async_launch(LobpcgAsync *a, cudaStream_t s);
 bool lobpcg_async_done(const LobpcgAsync *a);
 void lobpcg_async_finish(const LobpcgAsync *a, krans_request_result *out);
-void lobpcg_async_release(LobpcgAsync *a);
+void lobpcg_async_release(LobpcgAsync *a, std::vector<void *> *graveyard = nullptr);
 int lobpcg_async_cancel(LobpcgAsync *a, cudaStream_t ctl);
 } // namespace kr
 
 struct ServerTicket {
   krans_request req;
   int state = 0; // 0 queued, 1 running, 2 done, 3 failed, 4 cancelled
+  bool cancel_requested = false; // krans_cancel while running
   krans_request_result res;
   Clock::time_point submit_t, start_t, done_t;
 };
@@ -690,6 +692,14 @@ struct krans_server {
   std::vector<InFlight *> inflight;
   InFlight *open = nullptr; // the launch that takes new cyclic requests
   std::deque<uint64_t> completed; // finished tickets not yet handed out by krans_server_completed
+  std::vector<void *> graveyard;  // pinned host buffers of finished launches, freed once nothing runs
+  void bury_if_idle() {
+    if (!inflight.empty())
+      return;
+    for (void *h : graveyard)
+      cudaFreeHost(h);
+    graveyard.clear();
+  }
   size_t bytes_in_use = 0;
   uint64_t next_ticket = 1;
   int64_t next_launch = 1;
@@ -754,7 +764,7 @@ bool krans_server::admit_lobpcg(uint64_t id, Clock::time_point now) {
   rc = ew == cudaSuccess ? lobpcg_async_launch(a, streams[fs]) : cuda_fail(ew, "server stream order", __FILE__, __LINE__);
   queue.pop_front();
   if (rc != KRANS_OK) {
-    lobpcg_async_release(a);
+    lobpcg_async_release(a, &graveyard);
     fail(id, rc, now);
     return true;
   }
@@ -836,13 +846,19 @@ bool krans_server::admit_cyclic(Clock::time_point now) {
     f->L = BatchLaunch();
     rc = f->L.plan(ctx, rq.data(), (int)rq.size(), &need, true, opts.max_batch, floors);
   }
-  // the requests taken leave the queue (those that stayed keep their places)
-  for (auto id2 : take)
-    for (auto q = queue.begin(); q != queue.end(); ++q)
-      if (*q == id2) {
-        queue.erase(q);
-        break;
-      }
+  // the requests taken leave the queue (those that stayed keep their places):
+  // they are its first entries in order, with only cancelled ones between
+  for (size_t ti = 0; ti < take.size() && !queue.empty();) {
+    const uint64_t q0 = queue.front();
+    if (q0 == take[ti]) {
+      queue.pop_front();
+      ti++;
+    } else if (tickets[q0].state == 4) {
+      queue.pop_front();
+    } else {
+      break;
+    }
+  }
   if (rc != KRANS_OK) {
     for (auto id2 : take)
       fail(id2, rc, now);
@@ -870,7 +886,7 @@ bool krans_server::admit_cyclic(Clock::time_point now) {
   if (rc != KRANS_OK) {
     for (auto id2 : take)
       fail(id2, rc, now);
-    f->L.release();
+    f->L.release(&graveyard);
     delete f;
     return true;
   }
@@ -923,7 +939,7 @@ void krans_server::run() {
       if (f->lob) {
         lobpcg_async_finish(f->lob, &tickets[f->lob_ticket].res);
         finish(f->lob_ticket, now, f->id);
-        lobpcg_async_release(f->lob);
+        lobpcg_async_release(f->lob, &graveyard);
       } else {
         for (auto it = f->running.rbegin(); it != f->running.rend(); ++it) {
           ServerTicket &t = tickets[it->ticket];
@@ -931,15 +947,23 @@ void krans_server::run() {
             f->L.fill_slot(it->slot, &t.res);
             finish(it->ticket, now, f->id);
           } else if (!f->L.claimed(it->slot)) {
-            t.state = 0; // published after its launch's teams had left: queue it again
-            queue.push_front(it->ticket);
+            if (t.cancel_requested) { // cancelled before any team took it
+              memset(&t.res, 0, sizeof t.res);
+              t.res.status = KRANS_ERR_CANCELLED;
+              t.state = 4;
+              t.done_t = now;
+              completed.push_back(it->ticket);
+            } else {
+              t.state = 0; // published after its launch's teams had left: queue it again
+              queue.push_front(it->ticket);
+            }
           } else {
             fail(it->ticket, KRANS_ERR_RUNTIME, now);
           }
         }
         if (open == f)
           open = nullptr;
-        f->L.release();
+        f->L.release(&graveyard);
       }
       stream_busy[(size_t)f->stream_idx] = false;
       bytes_in_use -= std::min(bytes_in_use, f->bytes);
@@ -947,6 +971,7 @@ void krans_server::run() {
       inflight.erase(inflight.begin() + (long)i);
       moved = true;
     }
+    bury_if_idle();
     // 3) admission
     while (!queue.empty()) {
       const uint64_t id = queue.front();
@@ -994,6 +1019,16 @@ int krans_server_create(krans_ctx *ctx, const krans_server_opts *opts, krans_ser
   if (s->opts.max_batch < 1)
     s->opts.max_batch = 1;
   cudaError_t e = cudaSetDevice(ctx->device);
+  if (e == cudaSuccess) {
+    // launch workspaces come from the device's stream-ordered pool; keep what
+    // finished launches return there instead of giving it back to the driver
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, ctx->device) == cudaSuccess) {
+      uint64_t keep = ~0ull;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    cudaGetLastError();
+  }
   for (int i = 0; i < s->opts.max_inflight_launches && e == cudaSuccess; i++) {
     cudaStream_t st;
     e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
@@ -1043,6 +1078,10 @@ int krans_server_destroy(krans_server *s) {
       f->L.release();
     delete f;
   }
+  s->inflight.clear();
+  s->bury_if_idle();
+  for (auto st : s->streams)
+    cudaStreamSynchronize(st); // stream-ordered frees done before the streams go
   for (auto st : s->streams)
     cudaStreamDestroy(st);
   if (s->ctl)
@@ -1095,6 +1134,9 @@ int krans_cancel(krans_server *s, uint64_t ticket) {
   }
   if (it->second.state == 1) {
     // running: write the cancellation into the request's device status word
+    // (remembered too: a published request that no team claimed before its
+    // launch ended is not queued again)
+    it->second.cancel_requested = true;
     for (InFlight *f : s->inflight) {
       if (f->lob && f->lob_ticket == ticket)
         return lobpcg_async_cancel(f->lob, s->ctl);
@@ -1109,15 +1151,13 @@ int krans_cancel(krans_server *s, uint64_t ticket) {
     set_error("krans_cancel: ticket %llu has finished", (unsigned long long)ticket);
     return KRANS_ERR_RUNTIME;
   }
+  // queued: marked cancelled; the scheduler drops it when it reaches the
+  // queue's head or a batch being formed (no search of the queue here, which
+  // would make cancelling a long queue quadratic)
   it->second.state = 4;
   memset(&it->second.res, 0, sizeof it->second.res);
   it->second.res.status = KRANS_ERR_CANCELLED;
   s->completed.push_back(ticket);
-  for (auto q = s->queue.begin(); q != s->queue.end(); ++q)
-    if (*q == ticket) {
-      s->queue.erase(q);
-      break;
-    }
   return KRANS_OK;
 }
 

@@ -118,6 +118,8 @@ __device__ __noinline__ void run_cta_request(TeamShared *sh, CyclicDesc *dp, con
     d.trans_run = rq.trans_run;
     d.rng = rq.rng;
     d.initial_right = rq.initial_right;
+    d.nb_init = rq.nb_init;
+    d.frob_init = rq.frob_init;
     if (rq.basis) // else the basis stays in the workspace (own_basis)
       d.basis = rq.basis;
     d.ldb = rq.plan.ldb;
@@ -199,6 +201,8 @@ __device__ __noinline__ void run_cluster_request(TeamShared *sh, CyclicDesc *dp,
     d.trans_run = rq.trans_run;
     d.rng = rq.rng;
     d.initial_right = rq.initial_right;
+    d.nb_init = rq.nb_init;
+    d.frob_init = rq.frob_init;
     if (rq.basis) // else the basis stays in the workspace (own_basis)
       d.basis = rq.basis;
     d.ldb = rq.plan.ldb;

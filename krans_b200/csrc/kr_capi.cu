@@ -54,6 +54,30 @@ void dev_free(krans_ctx *ctx, void *p, size_t bytes) {
   ctx->in_use -= std::min(ctx->in_use, bytes);
 }
 
+int dev_alloc_async(krans_ctx *ctx, void **p, size_t bytes, cudaStream_t s) {
+  *p = nullptr;
+  if (bytes == 0)
+    bytes = 256;
+  if (ctx->budget && ctx->in_use + bytes > ctx->budget) {
+    set_error("HBM budget exceeded: %zu + %zu > %zu bytes", ctx->in_use, bytes, ctx->budget);
+    return KRANS_ERR_OUT_OF_MEMORY;
+  }
+  cudaError_t e = cudaMallocAsync(p, bytes, s);
+  if (e != cudaSuccess)
+    return cuda_fail(e, "cudaMallocAsync", __FILE__, __LINE__);
+  ctx->in_use += bytes;
+  return KRANS_OK;
+}
+
+void dev_free_async(krans_ctx *ctx, void *p, size_t bytes, cudaStream_t s) {
+  if (!p)
+    return;
+  if (bytes == 0)
+    bytes = 256;
+  cudaFreeAsync(p, s);
+  ctx->in_use -= std::min(ctx->in_use, bytes);
+}
+
 // Threads per row of the SpMV. Short rows go one per thread: the gathers of
 // these operators are random sectors, and a thread walking a short row keeps
 // the most of them in flight per instruction (measured on B200: the F^T of a
@@ -861,6 +885,7 @@ int krans_cyclic_opts_init(krans_cyclic_opts *o) {
   o->precond_aat = KRANS_PRECOND_NONE;
   o->precond_steps = 8;
   o->polish_block = 0;
+  o->mixed_fallback = 1;
   return KRANS_OK;
 }
 

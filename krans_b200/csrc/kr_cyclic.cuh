@@ -741,8 +741,8 @@ template <class Team, class KT> struct CyclicSolver {
 
   // candidate v = sum_q coef_q Y[q] (CyclicLanczosSolver.cpp:496-503)
   KR_DEV void form_candidate(const KT *Y, bool split, int l, int jb, int ny_used, double *v) {
-    if (threadIdx.x < (unsigned)ny_used)
-      tm.sh->h[threadIdx.x] = coef(split, l, jb, threadIdx.x);
+    for (int q = threadIdx.x; q < ny_used; q += blockDim.x)
+      tm.sh->h[q] = coef(split, l, jb, q);
     __syncthreads();
     const int64_t ldn = d.ldn;
     team_for4(tm, n, [&](const int64_t *ix, int cnt) {
@@ -936,7 +936,10 @@ template <class Team, class KT> struct CyclicSolver {
     bool converged = false;
 
     const uint64_t t_run0 = globaltimer_ns();
-    frob = fro_est();
+    // a continued run (the FP64 continuation of a mixed solve) keeps the
+    // estimate and the vectors its predecessor accepted
+    frob = d.frob_init > 0.0 ? d.frob_init : fro_est();
+    nb = d.nb_init;
     if (d.o.precond_aat == KRANS_PRECOND_JACOBI)
       jacobi_weights();
     const double fmx = fmax(1.0, frob);

@@ -1,8 +1,9 @@
 // Tall-skinny products of the block solver:
-//   team_gemm_tn:       C = A^T B (Gram matrices S = Z^T Z, G = Z^T (AZ),
-//                       Cholesky QR, projections), FP64 tensor cores: tiled
-//                       with shared-memory panels for long, wide products,
-//                       one warp per output tile otherwise
+//   team_gemm_tn:       C = A^T B (Cholesky QR of short blocks, projections),
+//                       FP64 tensor cores: shared-memory panels for long, wide
+//                       products (team_gemm_tn_panel), one warp per output
+//                       tile otherwise
+//   team_gram_sym_tiled: S = Z^T Z and G = Z^T (AZ), upper tiles, panels
 //   team_gram2_direct:  S = Z^T Z and G = Z^T (AZ) in one pass (short or
 //                       narrow blocks)
 //   team_gemm_nn:       out (-)= Z * Y[roff:roff+zc, 0:q] (n x q), FP64 tensor
@@ -20,124 +21,6 @@ KR_DEV void dmma_8x8x4(double &d0, double &d1, double a, double b) {
   asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
                : "+d"(d0), "+d"(d1)
                : "d"(a), "d"(b));
-}
-
-// C = A^T B (a x b, leading dim a) for tall-skinny column-major A (n x a) and
-// B (n x b), leading dim ld, on the FP64 tensor cores with shared-memory
-// panels. Work items are (64 x 64 tile of C, fixed chunk of rows); a block
-// stages 16-row panels of the tile's 64 columns of A and of B in shared
-// memory, and each of its 16 warps accumulates a 16 x 16 piece (four DMMA
-// 8x8 tiles). Each item leaves its partial tile in `part`; the partials are
-// then summed in chunk order, so the result depends only on the team size
-// (which fixes the chunking), not on which block ran which item. `part` must
-// hold ceil(a/64) * ceil(b/64) * 4096 * nchunks doubles, nchunks <= ncta.
-// Blocks of 512 threads.
-#define KR_GT 64 // tile edge
-#define KR_GK 16 // rows per shared-memory panel
-template <class Team>
-KR_DEV void team_gemm_tn_tiled(Team &tm, int64_t n, const double *A, int a, const double *B, int b, int64_t ld,
-                               double *C, double *part) {
-  __shared__ double sA[KR_GT][KR_GK + 1], sB[KR_GT][KR_GK + 1];
-  const int ta = (a + KR_GT - 1) / KR_GT, tb = (b + KR_GT - 1) / KR_GT, nt = ta * tb;
-  const int ncta = tm.ncta();
-  const int64_t kblocks = (n + KR_GK - 1) / KR_GK;
-  const int nch = (int)imin64(imin64(ncta, kblocks > 0 ? kblocks : 1), (int64_t)(2 * ncta + nt - 1) / nt);
-  const int nchunks = nch > 0 ? nch : 1;
-  const int64_t kb_per = (kblocks + nchunks - 1) / nchunks; // panels per chunk
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  const int wr = (wid >> 2) * 16, wc = (wid & 3) * 16; // this warp's 16 x 16 piece
-  const int items = nt * nchunks;
-  for (int it = tm.cta_rank(); it < items; it += ncta) {
-    const int tile = it % nt, ch = it / nt;
-    const int ti = tile % ta, tj = tile / ta;
-    const int64_t kb0 = (int64_t)ch * kb_per, kb1 = imin64(kb0 + kb_per, kblocks);
-    double acc[2][2][2];
-#pragma unroll
-    for (int x = 0; x < 2; x++)
-#pragma unroll
-      for (int y = 0; y < 2; y++)
-        acc[x][y][0] = acc[x][y][1] = 0.0;
-    // panels travel global -> registers two ahead of use -> shared memory, so
-    // their loads are in flight while the tensor cores work on the current one
-    constexpr int PER = (2 * KR_GT * KR_GK + 511) / 512; // elements per thread and panel (512 threads)
-    auto fetch = [&](int64_t kb, double (&v)[PER]) {
-      const int64_t r0 = kb * KR_GK;
-#pragma unroll
-      for (int q = 0; q < PER; q++) {
-        const int e = threadIdx.x + q * 512;
-        const int which = e / (KR_GT * KR_GK), rem = e % (KR_GT * KR_GK);
-        const int c = rem / KR_GK, k = rem % KR_GK;
-        const int64_t r = r0 + k;
-        double x = 0.0;
-        if (e < 2 * KR_GT * KR_GK && kb < kb1 && r < n) {
-          const int col = (which == 0 ? ti : tj) * KR_GT + c;
-          if (col < (which == 0 ? a : b))
-            x = (which == 0 ? A : B)[(int64_t)col * ld + r];
-        }
-        v[q] = x;
-      }
-    };
-    double v0[PER], v1[PER];
-    fetch(kb0, v0);
-    fetch(kb0 + 1, v1);
-    for (int64_t kb = kb0; kb < kb1; kb++) {
-#pragma unroll
-      for (int q = 0; q < PER; q++) {
-        const int e = threadIdx.x + q * 512;
-        if (e < 2 * KR_GT * KR_GK) {
-          const int which = e / (KR_GT * KR_GK), rem = e % (KR_GT * KR_GK);
-          const int c = rem / KR_GK, k = rem % KR_GK;
-          if (which == 0)
-            sA[c][k] = v0[q];
-          else
-            sB[c][k] = v0[q];
-        }
-        v0[q] = v1[q];
-      }
-      __syncthreads();
-      fetch(kb + 2, v1);
-      if (wid < 16) {
-#pragma unroll
-        for (int kk = 0; kk < KR_GK; kk += 4) {
-          double fa[2], fb[2];
-#pragma unroll
-          for (int x = 0; x < 2; x++)
-            fa[x] = sA[wr + 8 * x + (lane >> 2)][kk + (lane & 3)];
-#pragma unroll
-          for (int y = 0; y < 2; y++)
-            fb[y] = sB[wc + 8 * y + (lane >> 2)][kk + (lane & 3)];
-#pragma unroll
-          for (int x = 0; x < 2; x++)
-#pragma unroll
-            for (int y = 0; y < 2; y++)
-              dmma_8x8x4(acc[x][y][0], acc[x][y][1], fa[x], fb[y]);
-        }
-      }
-      __syncthreads();
-    }
-    if (wid < 16) {
-      double *pt = part + (size_t)it * (KR_GT * KR_GT);
-#pragma unroll
-      for (int x = 0; x < 2; x++)
-#pragma unroll
-        for (int y = 0; y < 2; y++) {
-          const int i = wr + 8 * x + (lane >> 2), j = wc + 8 * y + 2 * (lane & 3);
-          pt[i + j * KR_GT] = acc[x][y][0];
-          pt[i + (j + 1) * KR_GT] = acc[x][y][1];
-        }
-    }
-  }
-  tm.sync();
-  const int64_t nthr = tm.nthreads();
-  for (int64_t e = tm.tid(); e < (int64_t)a * b; e += nthr) {
-    const int i = (int)(e % a), j = (int)(e / a);
-    const int tile = (i / KR_GT) + ta * (j / KR_GT), li = i % KR_GT, lj = j % KR_GT;
-    double s = 0.0;
-    for (int ch = 0; ch < nchunks; ch++)
-      s += __ldcg(part + (size_t)(tile + ch * nt) * (KR_GT * KR_GT) + li + lj * KR_GT);
-    C[e] = s;
-  }
-  tm.sync();
 }
 
 // C = A^T B for tall-skinny A (n x a) and B (n x b), column-major with
@@ -288,7 +171,8 @@ KR_DEV void team_gram2_direct(Team &tm, int64_t n, const double *Z, const double
 // depends only on the team size. `part` must hold (2 ncta + tiles) * 8192
 // doubles; needs 512 threads and gram_tiled_smem_bytes() of dynamic shared
 // memory.
-#define KR_GP 32 // rows per panel of the tiled Gram
+#define KR_GT 64 // tile edge of the panel products
+#define KR_GP 32 // rows per panel of the panel products
 __host__ __device__ constexpr size_t gram_tiled_smem_bytes() { return (size_t)3 * KR_GT * (KR_GP + 1) * 8; }
 
 template <class Team>
@@ -419,6 +303,112 @@ KR_DEV void team_gram_sym_tiled(Team &tm, int64_t n, const double *Z, const doub
   tm.sync();
 }
 
+// C = A^T B (a x b, leading dim a) for long, wide products: the general form
+// of team_gram_sym_tiled. Work items are (64 x 64 tile of C, fixed chunk of
+// rows); a block stages 32-row panels of the tile's columns of A and of B in
+// shared memory, fetching the next panel into registers while the current
+// one is multiplied, and each of its 16 warps accumulates a 16 x 16 piece of
+// the tile (2 x 2 DMMA 8x8 tiles). Partial tiles are summed in chunk order,
+// so the result depends only on the team size. `part` must hold
+// (2 ncta + tiles) * 4096 doubles, tiles = ceil(a/64) * ceil(b/64); needs 512
+// threads and gram_tiled_smem_bytes() of dynamic shared memory.
+template <class Team>
+KR_DEV void team_gemm_tn_panel(Team &tm, int64_t n, const double *A, int a, const double *B, int b, int64_t ld,
+                               double *C, double *part) {
+  extern __shared__ __align__(16) double kr_gemm_smem[];
+  typedef double Panel[KR_GP + 1];
+  Panel *sA = reinterpret_cast<Panel *>(kr_gemm_smem);
+  Panel *sB = sA + KR_GT;
+  const int ta = (a + KR_GT - 1) / KR_GT, tb = (b + KR_GT - 1) / KR_GT, tiles = ta * tb;
+  const int ncta = tm.ncta();
+  const int64_t kblocks = (n + KR_GP - 1) / KR_GP;
+  const int nch = (int)imin64(imin64(ncta, kblocks > 0 ? kblocks : 1), (int64_t)(2 * ncta + tiles - 1) / tiles);
+  const int nchunks = nch > 0 ? nch : 1;
+  const int64_t kb_per = (kblocks + nchunks - 1) / nchunks;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int wr = (wid >> 2) * 16, wc = (wid & 3) * 16;
+  const int items = tiles * nchunks;
+  constexpr int PER = 2 * KR_GT * KR_GP / 512; // elements per thread and panel (two operands)
+  for (int it = tm.cta_rank(); it < items; it += ncta) {
+    const int tile = it % tiles, ch = it / tiles;
+    const int ti = tile % ta, tj = tile / ta;
+    const int64_t kb0 = (int64_t)ch * kb_per, kb1 = imin64(kb0 + kb_per, kblocks);
+    double acc[2][2][2];
+#pragma unroll
+    for (int x = 0; x < 2; x++)
+#pragma unroll
+      for (int y = 0; y < 2; y++)
+        acc[x][y][0] = acc[x][y][1] = 0.0;
+    double v[PER];
+    auto fetch = [&](int64_t kb) {
+      const int64_t r0 = kb * KR_GP;
+#pragma unroll
+      for (int q = 0; q < PER; q++) {
+        const int e = threadIdx.x + q * 512;
+        const int which = e / (KR_GT * KR_GP), rem = e % (KR_GT * KR_GP);
+        const int c = rem / KR_GP, k = rem % KR_GP;
+        const int64_t r = r0 + k;
+        double x = 0.0;
+        if (kb < kb1 && r < n) {
+          const int colx = (which == 0 ? ti : tj) * KR_GT + c;
+          if (colx < (which == 0 ? a : b))
+            x = (which == 0 ? A : B)[(int64_t)colx * ld + r];
+        }
+        v[q] = x;
+      }
+    };
+    fetch(kb0);
+    for (int64_t kb = kb0; kb < kb1; kb++) {
+#pragma unroll
+      for (int q = 0; q < PER; q++) {
+        const int e = threadIdx.x + q * 512;
+        const int which = e / (KR_GT * KR_GP), rem = e % (KR_GT * KR_GP);
+        (which == 0 ? sA : sB)[rem / KR_GP][rem % KR_GP] = v[q];
+      }
+      __syncthreads();
+      if (kb + 1 < kb1)
+        fetch(kb + 1);
+#pragma unroll
+      for (int kk = 0; kk < KR_GP; kk += 4) {
+        double fa[2], fb[2];
+#pragma unroll
+        for (int x = 0; x < 2; x++)
+          fa[x] = sA[wr + 8 * x + (lane >> 2)][kk + (lane & 3)];
+#pragma unroll
+        for (int y = 0; y < 2; y++)
+          fb[y] = sB[wc + 8 * y + (lane >> 2)][kk + (lane & 3)];
+#pragma unroll
+        for (int x = 0; x < 2; x++)
+#pragma unroll
+          for (int y = 0; y < 2; y++)
+            dmma_8x8x4(acc[x][y][0], acc[x][y][1], fa[x], fb[y]);
+      }
+      __syncthreads();
+    }
+    double *pt = part + (size_t)it * (KR_GT * KR_GT);
+#pragma unroll
+    for (int x = 0; x < 2; x++)
+#pragma unroll
+      for (int y = 0; y < 2; y++) {
+        const int i = wr + 8 * x + (lane >> 2), j = wc + 8 * y + 2 * (lane & 3);
+        pt[i + j * KR_GT] = acc[x][y][0];
+        pt[i + (j + 1) * KR_GT] = acc[x][y][1];
+      }
+  }
+  tm.sync();
+  const int64_t nthr = tm.nthreads();
+  for (int64_t e = tm.tid(); e < (int64_t)a * b; e += nthr) {
+    const int i = (int)(e % a), j = (int)(e / a);
+    const int ti = i / KR_GT, tj = j / KR_GT, li = i % KR_GT, lj = j % KR_GT;
+    const int tile = tj * ta + ti;
+    double sv = 0.0;
+    for (int ch = 0; ch < nchunks; ch++)
+      sv += __ldcg(part + (size_t)(tile + ch * tiles) * (KR_GT * KR_GT) + li + lj * KR_GT);
+    C[i + (size_t)j * a] = sv;
+  }
+  tm.sync();
+}
+
 // C = A^T B: the tiled kernel for long products with wide blocks, where the
 // shared-memory panels pay off; the direct one (one warp per 8 x 8 tile,
 // operands straight from global memory) for short or narrow ones, where
@@ -429,7 +419,7 @@ template <class Team>
 KR_DEV void team_gemm_tn(Team &tm, int64_t n, const double *A, int a, const double *B, int b, int64_t ld,
                          double *C, double *part) {
   if (n >= 131072 && (a >= 32 || b >= 32))
-    team_gemm_tn_tiled(tm, n, A, a, B, b, ld, C, part);
+    team_gemm_tn_panel(tm, n, A, a, B, b, ld, C, part);
   else
     team_gemm_tn_direct(tm, n, A, a, B, b, ld, C, part);
 }
@@ -450,9 +440,44 @@ KR_DEV void team_gemm_tn(Team &tm, int64_t n, const double *A, int a, const doub
 #define KR_NK 16  // k per chunk
 __host__ __device__ constexpr size_t gemm_nn_smem_bytes() { return (size_t)(KR_NT + KR_NQ) * (KR_NK + 1) * 8; }
 
+// Narrow form (q <= KR_NQ_DIRECT outputs): every thread takes whole rows and
+// sums over k in order on the CUDA cores, with no shared memory and no
+// barrier. For the few-column blocks of small solves the tiled form spends
+// two block barriers per 64-row tile on a 64 x 128 output group it barely
+// fills; this form costs none (the caller's barrier publishes the result).
+#define KR_NQ_DIRECT 16
+template <class Team>
+KR_DEV void team_gemm_nn_direct(Team &tm, int64_t n, const double *Z, int64_t ld, int zc, const double *Y, int ldy,
+                                int roff, int q, double *out, bool subtract) {
+  for (int64_t i = tm.tid(); i < n; i += tm.nthreads()) {
+    double acc[KR_NQ_DIRECT];
+#pragma unroll
+    for (int j = 0; j < KR_NQ_DIRECT; j++)
+      acc[j] = 0.0;
+    for (int k = 0; k < zc; k++) {
+      const double z = Z[(int64_t)k * ld + i];
+      const double *yk = Y + roff + k;
+#pragma unroll
+      for (int j = 0; j < KR_NQ_DIRECT; j++)
+        if (j < q)
+          acc[j] += z * yk[(int64_t)j * ldy];
+    }
+#pragma unroll
+    for (int j = 0; j < KR_NQ_DIRECT; j++)
+      if (j < q) {
+        double *o = out + (int64_t)j * ld + i;
+        *o = subtract ? *o - acc[j] : acc[j];
+      }
+  }
+}
+
 template <class Team>
 KR_DEV void team_gemm_nn(Team &tm, int64_t n, const double *Z, int64_t ld, int zc, const double *Y, int ldy,
                          int roff, int q, double *out, bool subtract) {
+  if (q <= KR_NQ_DIRECT) {
+    team_gemm_nn_direct(tm, n, Z, ld, zc, Y, ldy, roff, q, out, subtract);
+    return;
+  }
   extern __shared__ __align__(16) double kr_gemm_smem[];
   double(*sZ)[KR_NK + 1] = reinterpret_cast<double(*)[KR_NK + 1]>(kr_gemm_smem);
   double(*sY)[KR_NK + 1] = reinterpret_cast<double(*)[KR_NK + 1]>(kr_gemm_smem + KR_NT * (KR_NK + 1));

@@ -114,6 +114,12 @@ int spmv_rows_per_block(int64_t rows, int64_t nnz);
 // allocation with budget accounting
 int dev_alloc(krans_ctx *ctx, void **p, size_t bytes);
 void dev_free(krans_ctx *ctx, void *p, size_t bytes);
+// Stream-ordered forms (cudaMallocAsync / cudaFreeAsync on `s`): neither
+// waits for kernels running on other streams, unlike cudaFree, which waits
+// for the whole device. The served paths use them so that releasing one
+// finished launch never waits for a persistent launch still resident.
+int dev_alloc_async(krans_ctx *ctx, void **p, size_t bytes, cudaStream_t s);
+void dev_free_async(krans_ctx *ctx, void *p, size_t bytes, cudaStream_t s);
 int pick_lanes(int64_t rows, int64_t nnz);
 // threads per row of the solvers' SpMV from the context's tuning table
 inline int tuned_lanes(const krans_ctx *ctx, int64_t rows, int64_t nnz) {

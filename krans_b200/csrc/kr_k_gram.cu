@@ -1,7 +1,8 @@
-// Kernel TU: the block solver's two dense products on raw device arrays
-// (krans_block_gram, krans_block_combine): the same device code as inside
-// the LOBPCG kernel (team_gram_sym_tiled, team_gemm_nn), run by every block
-// of a cooperative launch, so that they can be tested and timed on their own.
+// Kernel TU: the block solver's dense products on raw device arrays
+// (krans_block_gram, krans_block_gemm_tn, krans_block_combine): the same
+// device code as inside the LOBPCG kernel (team_gram_sym_tiled, team_gemm_tn,
+// team_gemm_nn), run by every block of a cooperative launch, so that they can
+// be tested and timed on their own.
 #include <algorithm>
 
 #include "kr_gram.cuh"
@@ -15,6 +16,14 @@ __global__ void __launch_bounds__(512) block_gram_kernel(int64_t n, const double
   __shared__ TeamShared sh;
   TeamGrid tm{&sh, status, gb, gpart, 0, 0};
   team_gram_sym_tiled(tm, n, Z, W, ld, p, S, G, part);
+}
+
+__global__ void __launch_bounds__(512) block_gemm_tn_kernel(int64_t n, const double *A, int a, const double *B,
+                                                            int b, int64_t ld, double *C, double *part,
+                                                            GridBarrierState *gb, double *gpart, int *status) {
+  __shared__ TeamShared sh;
+  TeamGrid tm{&sh, status, gb, gpart, 0, 0};
+  team_gemm_tn(tm, n, A, a, B, b, ld, C, part);
 }
 
 __global__ void __launch_bounds__(512) block_combine_kernel(int64_t n, const double *Z, int64_t ld, int zc,
@@ -125,6 +134,49 @@ extern "C" int krans_block_gram(krans_ctx *ctx, int64_t n, int64_t p, const doub
     return cuda_fail(e, "krans_block_gram", __FILE__, __LINE__);
   if (h_status != 0) {
     set_error("krans_block_gram: device status %d (a bounded grid barrier gave up)", h_status);
+    return h_status;
+  }
+  return KRANS_OK;
+}
+
+extern "C" int krans_block_gemm_tn(krans_ctx *ctx, int64_t n, int64_t a, const double *A, int64_t b,
+                                   const double *B, int64_t ld, double *C, double *device_ms) {
+  KR_CHECK_ARG(ctx && A && B && C, "krans_block_gemm_tn: NULL argument");
+  KR_CHECK_ARG(n >= 0 && a >= 1 && b >= 1 && a <= 4096 && b <= 4096 && ld >= n,
+               "krans_block_gemm_tn: need n >= 0, 1 <= a, b <= 4096, ld >= n");
+  KR_CUDA(cudaSetDevice(ctx->device));
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  const void *k = (const void *)block_gemm_tn_kernel;
+  const int blocks = coop_blocks(k, ctx, gram_tiled_smem_bytes());
+  // partials of both forms: the panel form's (2 blocks + tiles) 64 x 64 tiles,
+  // the direct form's a x b per block
+  const int64_t tiles = ((a + KR_GT - 1) / KR_GT) * ((b + KR_GT - 1) / KR_GT);
+  const size_t part = std::max<size_t>((size_t)(2 * blocks + tiles) * KR_GT * KR_GT, (size_t)blocks * a * b);
+  char *ws = nullptr;
+  size_t bytes = 0;
+  GridBarrierState *gb;
+  double *gpart, *pt;
+  int *status;
+  int rc = coop_scratch(ctx, blocks, part, &ws, &bytes, &gb, &gpart, &status, &pt);
+  if (rc != KRANS_OK)
+    return rc;
+  cudaStream_t s = ctx->stream;
+  cudaError_t e = cudaMemsetAsync(gb, 0, sizeof(GridBarrierState), s);
+  if (e == cudaSuccess)
+    e = cudaMemsetAsync(status, 0, sizeof(int), s);
+  int ai = (int)a, bi = (int)b;
+  void *args[] = {(void *)&n, (void *)&A, (void *)&ai, (void *)&B, (void *)&bi, (void *)&ld, (void *)&C,
+                  (void *)&pt, (void *)&gb, (void *)&gpart, (void *)&status};
+  if (e == cudaSuccess)
+    e = timed_coop(k, blocks, args, gram_tiled_smem_bytes(), s, device_ms);
+  int h_status = 0;
+  if (e == cudaSuccess)
+    e = cudaMemcpy(&h_status, status, sizeof(int), cudaMemcpyDeviceToHost);
+  dev_free(ctx, ws, bytes);
+  if (e != cudaSuccess)
+    return cuda_fail(e, "krans_block_gemm_tn", __FILE__, __LINE__);
+  if (h_status != 0) {
+    set_error("krans_block_gemm_tn: device status %d (a bounded grid barrier gave up)", h_status);
     return h_status;
   }
   return KRANS_OK;

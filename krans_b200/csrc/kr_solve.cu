@@ -48,14 +48,23 @@ static int cyclic_targets(const krans_cyclic_opts &o, int64_t m, int64_t n, int6
 struct RunOut {
   CyclicDevResult r;
   double ms;
+  int32_t fp64_fallback = 0; // the mixed run continued in FP64
+  int64_t fallback_from = 0; // vectors the mixed run had accepted
 };
 
 // One find_right_nullspace run on the device (a grid team, or one thread
 // block through the persistent batched kernel with a single request); the
 // basis rows are copied into new vectors owned by the caller.
+// `prefill` (nprefill rows, stride round_up(n, 32)) and `frob_init` continue
+// an earlier run: its accepted vectors are copied into the basis first and
+// its ||A||_F estimate is kept. A MIXED run that stops short of k_target with
+// its FP64 polish at cg_maxit continues that way in FP64 (o.mixed_fallback):
+// the FP32 recurrence's Ritz vectors were too far from the null space for
+// the projector to finish, which an FP64 recurrence avoids.
 static int run_cyclic(krans_ctx *ctx, const krans_mat *A, bool trans, krans_rng *rng,
                       const krans_cyclic_opts &o, const double *init_right, int64_t k_target,
-                      int64_t ncv, std::vector<krans_vec *> &found, RunOut *out) {
+                      int64_t ncv, std::vector<krans_vec *> &found, RunOut *out,
+                      const double *prefill = nullptr, int64_t nprefill = 0, double frob_init = 0.0) {
   const CsrView F = view_of(A, trans), B = view_of(A, !trans);
   const bool mixed = o.precision == KRANS_PREC_MIXED;
   if (mixed && !A->v32) {
@@ -134,6 +143,8 @@ static int run_cyclic(krans_ctx *ctx, const krans_mat *A, bool trans, krans_rng 
     d.trans_run = trans ? 1 : 0;
     d.rng = rng->d;
     d.initial_right = init_right;
+    d.nb_init = nprefill;
+    d.frob_init = frob_init;
     d.status = d_status;
     d.res = d_res;
     if (e == cudaSuccess)
@@ -150,11 +161,16 @@ static int run_cyclic(krans_ctx *ctx, const krans_mat *A, bool trans, krans_rng 
     q.status = d_status;
     q.max_resid = d_mr;
     q.initial_right = init_right;
+    q.nb_init = nprefill;
+    q.frob_init = frob_init;
     q.trivial = 0;
     q.trans_run = trans ? 1 : 0;
     if (e == cudaSuccess)
       e = cudaMemcpyAsync(d_req, &q, sizeof q, cudaMemcpyHostToDevice, s);
   }
+  if (e == cudaSuccess && nprefill > 0)
+    e = cudaMemcpy2DAsync(grid ? d.basis : basis, (size_t)p.ldb * 8, prefill, (size_t)p.ldb * 8, (size_t)p.n * 8,
+                          (size_t)nprefill, cudaMemcpyDeviceToDevice, s);
   if (e == cudaSuccess)
     e = cudaEventRecord(e0, s);
   if (e == cudaSuccess)
@@ -186,6 +202,31 @@ static int run_cyclic(krans_ctx *ctx, const krans_mat *A, bool trans, krans_rng 
     return out->r.status;
   }
   const double *bsrc = grid ? d.basis : basis;
+  if (mixed && o.mixed_fallback && !out->r.converged && out->r.n_found < k_target && out->r.cg_maxit_hits > 0) {
+    krans_cyclic_opts o64 = o;
+    o64.precision = KRANS_PREC_FP64;
+    RunOut o2;
+    rc = run_cyclic(ctx, A, trans, rng, o64, init_right, k_target, ncv, found, &o2, bsrc, out->r.n_found,
+                    out->r.frob);
+    dev_free(ctx, ws, bytes);
+    if (rc != KRANS_OK)
+      return rc;
+    const CyclicDevResult r1 = out->r;
+    out->fallback_from = r1.n_found;
+    out->fp64_fallback = 1;
+    out->r = o2.r;
+    out->r.restarts += r1.restarts;
+    out->r.krylov_steps_total += r1.krylov_steps_total;
+    out->r.cg_solves += r1.cg_solves;
+    out->r.cg_maxit_hits += r1.cg_maxit_hits;
+    out->r.spmv += r1.spmv;
+    out->r.spmvT += r1.spmvT;
+    out->r.bytes += r1.bytes;
+    for (int q2 = 0; q2 < 4; q2++)
+      out->r.phase_ms[q2] += r1.phase_ms[q2];
+    out->ms += o2.ms;
+    return KRANS_OK;
+  }
   rc = KRANS_OK;
   for (int64_t i = 0; i < out->r.n_found && rc == KRANS_OK; i++) {
     krans_vec *v = nullptr;
@@ -249,6 +290,8 @@ extern "C" int krans_solve_cyclic(krans_ctx *ctx, const krans_mat *A, krans_rng 
     result->device_ms = ro.ms;
     for (int q = 0; q < 4; q++)
       result->phase_ms[q] = ro.r.phase_ms[q];
+    result->fp64_fallback = ro.fp64_fallback;
+    result->fallback_from = (int32_t)ro.fallback_from;
   }
   for (size_t i = 0; i < right.size(); i++)
     right_out[i] = right[i];
@@ -280,6 +323,7 @@ extern "C" int krans_solve_cyclic(krans_ctx *ctx, const krans_mat *A, krans_rng 
     lo.polish_block = o.polish_block;
     lo.precond_aat = o.precond_aat;
     lo.precond_steps = o.precond_steps;
+    lo.mixed_fallback = o.mixed_fallback;
     if (o.rank_known >= 0) {
       const int left_nullity = (int)A->m - o.rank_known;
       lo.nullity_known = std::max(0, std::min(left_nullity, (int)o.k));
@@ -297,6 +341,7 @@ extern "C" int krans_solve_cyclic(krans_ctx *ctx, const krans_mat *A, krans_rng 
         result->spmvT += ro.r.spmvT;
         result->algo_bytes += ro.r.bytes;
         result->device_ms += ro.ms;
+        result->fp64_fallback |= ro.fp64_fallback;
       }
     }
     for (size_t i = 0; i < left.size(); i++)

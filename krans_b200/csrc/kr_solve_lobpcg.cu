@@ -336,6 +336,7 @@ struct LobpcgAsync {
   LobpcgDevResult *h_res = nullptr;
   double *h_mr = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, evd = nullptr;
+  cudaStream_t stream = nullptr; // the launch's stream (stream-ordered workspace)
 };
 
 static void seed_state(RngState &s, uint32_t seed, int mode) {
@@ -427,9 +428,10 @@ int lobpcg_async_plan(krans_ctx *ctx, const krans_request &r, LobpcgAsync **out,
 int lobpcg_async_launch(LobpcgAsync *a, cudaStream_t s) {
   if (a->trivial)
     return KRANS_OK;
-  int rc = dev_alloc(a->ctx, (void **)&a->ws, a->bytes);
+  int rc = dev_alloc_async(a->ctx, (void **)&a->ws, a->bytes, s);
   if (rc != KRANS_OK)
     return rc;
+  a->stream = s;
   char *p = a->ws;
   LobpcgDesc &d = a->d;
   d.rng = nullptr;
@@ -527,15 +529,20 @@ int lobpcg_async_cancel(LobpcgAsync *a, cudaStream_t ctl) {
   return e == cudaSuccess ? KRANS_OK : cuda_fail(e, "cancel request", __FILE__, __LINE__);
 }
 
-void lobpcg_async_release(LobpcgAsync *a) {
+// Pinned host buffers go to `graveyard` when one is given (cudaFreeHost
+// waits for the whole device; the server frees them once nothing runs).
+void lobpcg_async_release(LobpcgAsync *a, std::vector<void *> *graveyard) {
   if (!a)
     return;
   if (a->ws)
-    dev_free(a->ctx, a->ws, a->bytes);
-  if (a->h_res)
-    cudaFreeHost(a->h_res);
-  if (a->h_mr)
-    cudaFreeHost(a->h_mr);
+    dev_free_async(a->ctx, a->ws, a->bytes, a->stream);
+  for (void *h : {(void *)a->h_res, (void *)a->h_mr})
+    if (h) {
+      if (graveyard)
+        graveyard->push_back(h);
+      else
+        cudaFreeHost(h);
+    }
   if (a->ev0)
     cudaEventDestroy(a->ev0);
   if (a->ev1)

@@ -63,6 +63,8 @@ struct CyclicDesc {
   RngState *rng;
   const double *initial_right; // n doubles or nullptr
   double *basis;               // k_target x ldn (output, row i = vector i)
+  int64_t nb_init;             // rows of basis already accepted (a continued run), else 0
+  double frob_init;            // ||A||_F estimate of the run being continued, else 0 (estimate it)
   void *Y, *X, *wx, *wy;       // KT storage
   double *y0, *v, *vp, *best_v, *tn; // n-vectors
   double *Vc;                        // KR_NBP candidate n-vectors (block polish)
@@ -197,6 +199,8 @@ struct CyclicRequestDev {
   int32_t *status;
   double *max_resid;
   const double *initial_right; // start vector y0 or nullptr
+  int64_t nb_init;             // basis rows already accepted (continued run), else 0
+  double frob_init;            // ||A||_F estimate to reuse (continued run), else 0
   HostDone *done;              // open launches: completion record (else nullptr)
   int32_t trivial;   // reference early exit: nothing to compute
   int32_t trans_run; // 1: the run is on A^T (left null space)

@@ -1,7 +1,9 @@
 """The block solver's dense products on their own (krans_block_gram,
-krans_block_combine: the device code LOBPCG runs inside its kernel) against
-numpy: S = Z^T Z and G = Z^T W formed on the upper triangle and mirrored, as
-the reference's form_gram does (LOBPCGSolver.cpp:67-80), and out = Z C as
+krans_block_gemm_tn, krans_block_combine: the device code LOBPCG runs inside
+its kernel) against numpy: S = Z^T Z and G = Z^T W formed on the upper
+triangle and mirrored, as the reference's form_gram does
+(LOBPCGSolver.cpp:67-80), C = A^T B as the basis projections of
+orthonormalize_block (LOBPCGSolver.cpp:137-160), and out = Z C as
 combine_columns (LOBPCGSolver.cpp:122-134). Tolerance: 64 ulp of the sum of
 absolute products of each entry."""
 import numpy as np
@@ -43,6 +45,30 @@ def test_block_gram(ctx, n, p):
     assert torch.equal(S2, S)
 
 
+@pytest.mark.parametrize("n,a,b", [(1, 1, 1), (1000, 5, 3), (131_072, 64, 96), (300_001, 40, 7),
+                                   (200_000, 130, 70)])
+def test_block_gemm_tn(ctx, n, a, b):
+    # n >= 131072 with a or b >= 32: the shared-memory panel form; else one
+    # warp per 8 x 8 output tile
+    import torch
+    import krans_b200 as kb
+    rng = np.random.default_rng(n + a + b)
+    ld = n + 5
+    Ac, Bc = rng.standard_normal((a, ld)), rng.standard_normal((b, ld))
+    A, B = dev(Ac), dev(Bc)
+    Cd = torch.full((b, a), 3.0, dtype=torch.float64, device="cuda:0")
+    torch.cuda.synchronize()
+    kb.block_gemm_tn(ctx, n, a, A.data_ptr(), b, B.data_ptr(), ld, Cd.data_ptr())
+    An, Bn = Ac[:, :n].T, Bc[:, :n].T
+    ref = An.T @ Bn
+    tol = 64 * EPS * (np.abs(An).T @ np.abs(Bn))
+    got = Cd.cpu().numpy().T  # column-major a x b
+    assert np.all(np.abs(got - ref) <= tol)
+    C2 = torch.zeros_like(Cd)
+    kb.block_gemm_tn(ctx, n, a, A.data_ptr(), b, B.data_ptr(), ld, C2.data_ptr())
+    assert torch.equal(C2, Cd)  # deterministic
+
+
 @pytest.mark.parametrize("n,zc,q", [(1, 1, 1), (1000, 3, 3), (200_001, 96, 96), (70_000, 288, 96), (5000, 40, 300)])
 def test_block_combine(ctx, n, zc, q):
     import torch
@@ -73,3 +99,5 @@ def test_block_products_invalid(ctx):
         kb.block_gram(ctx, 10, 3, 16, 10, 16, W=16)  # W without G
     with pytest.raises(ValueError):
         kb.block_combine(ctx, 10, 3, 2, 16, 10, 16, 2, 16)  # ldc < zc
+    with pytest.raises(ValueError):
+        kb.block_gemm_tn(ctx, 10, 3, 16, 2, 16, 9, 16)  # ld < n

@@ -136,7 +136,11 @@ def test_cyclic_planted_mixed_vs_fp64_oracle(ctx, oracle, k, ncv):
     # The planted-kernel workload A = [B | B W] at 1/1000 of its size: the
     # mixed-precision form (FP32 SpMV and Lanczos recurrence, FP64
     # reorthogonalisation, tiny SVD and CG polish) against the FP64 oracle on
-    # the same input and start vectors, vector by vector.
+    # the same input and start vectors, vector by vector. A A^T is
+    # ill-conditioned here, so the FP64 polish cannot finish the FP32 Ritz
+    # vectors within cg_maxit = 1000; the solve continues in FP64 from the
+    # vectors it had accepted (mixed_fallback) and must then meet the same
+    # bound as an FP64 solve.
     import krans_b200 as kb
     inst = G.planted_kernel(3000, 2000, k, seed=2)
     A = inst.A
@@ -148,7 +152,12 @@ def test_cyclic_planted_mixed_vs_fp64_oracle(ctx, oracle, k, ncv):
     U = kb.basis_to_numpy(R.right_null)
     O = oracle.cyclic(oracle.Csr.from_scipy(A), oracle.Rng(42), **opt)
     assert R.converged_to_target and O.converged_to_target
-    check_basis(oracle, A, U, O.right_null, inst.kernel)
+    assert R.fp64_fallback and 0 <= R.fallback_from < k
+    check_basis(oracle, A, U, O.right_null)
+    # the planted basis (columns of [W; -I_k], W sparse) has exact zeros, which make its pivoted RREF
+    # ill-posed (pivot choices flip under rounding): compared by subspace
+    # distance only (the RREF compare against the oracle's basis holds above)
+    assert oracle.subspace_dist(inst.kernel, U) <= DIST
     # per vector: distance of each mixed-precision vector from the FP64 basis
     P = O.right_null
     per_vec = np.linalg.norm(U - (U @ P.T) @ P, axis=1)
