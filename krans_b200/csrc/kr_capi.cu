@@ -246,6 +246,25 @@ __global__ void rng_philox_kernel(RngState *st, double *out, int64_t n) {
 }
 __global__ void rng_philox_advance(RngState *st, int64_t n) { st->philox_ctr += (uint64_t)n; }
 
+void preload(const void *kernel) {
+  cudaFuncAttributes a;
+  if (cudaFuncGetAttributes(&a, kernel) != cudaSuccess)
+    cudaGetLastError();
+}
+
+void preload_capi_kernels() {
+  const void *ks[] = {(const void *)dot_partial_kernel, (const void *)sum_partials_kernel,
+                      (const void *)axpy_kernel,        (const void *)scale_kernel,
+                      (const void *)scale_by_inv_norm_kernel, (const void *)fill_kernel,
+                      (const void *)to_f32_kernel,      (const void *)col_count_kernel,
+                      (const void *)scan_kernel,        (const void *)scatter_kernel,
+                      (const void *)row_sort_kernel,    (const void *)row_of_kernel,
+                      (const void *)gather_t_kernel,    (const void *)rng_mt_kernel,
+                      (const void *)rng_philox_kernel,  (const void *)rng_philox_advance};
+  for (const void *k : ks)
+    preload(k);
+}
+
 static int grid_for(krans_ctx *ctx, int64_t n, int threads = 256) {
   int64_t b = (n + threads - 1) / threads;
   const int64_t cap = (int64_t)ctx->sms * 8;
@@ -303,6 +322,15 @@ int krans_ctx_create(int device, size_t hbm_budget_bytes, krans_ctx **out) {
     krans_ctx_destroy(c);
     return rc;
   }
+  preload_capi_kernels();
+  preload_spmv_kernels();
+  preload_gram_kernels();
+  preload_batch_cta_kernels();
+  preload_batch_cluster_kernels();
+  preload_cyclic_grid_kernels();
+  preload_lobpcg_kernels();
+  preload_lobpcg_cta_kernels();
+  preload_lobpcg_cluster_kernels();
   *out = c;
   return KRANS_OK;
 }

@@ -240,8 +240,23 @@ KR_DEV double blk_allsum(double v, double *red) {
 
 #define KR_EIG_MAX 512
 
+// Thread groups of the eigensolver: the whole block, or warp 0 alone (small
+// pencils, where block barriers dominate: the same steps with warp barriers).
+struct EigBlock {
+  KR_DEV static int tid() { return threadIdx.x; }
+  KR_DEV static int size() { return blockDim.x; }
+  KR_DEV static void sync() { __syncthreads(); }
+  KR_DEV static double allsum(double v, double *red) { return blk_allsum(v, red); }
+};
+struct EigWarp { // called by warp 0 only
+  KR_DEV static int tid() { return threadIdx.x & 31; }
+  KR_DEV static int size() { return 32; }
+  KR_DEV static void sync() { __syncwarp(); }
+  KR_DEV static double allsum(double v, double *) { return warp_sum(v); }
+};
+
 // Symmetric eigendecomposition of A (n x n, column-major, ld n; both
-// triangles referenced, destroyed) on one thread block: Householder reduction
+// triangles referenced, destroyed) on a thread group: Householder reduction
 // to tridiagonal form with the orthogonal factor accumulated explicitly, then
 // the implicit QL algorithm with shifts for the tridiagonal matrix (Golub &
 // Van Loan, Matrix Computations, 4th ed., 8.3.1 and 8.3.3; QL as in Bowdler,
@@ -251,13 +266,13 @@ KR_DEV double blk_allsum(double v, double *red) {
 // independent). w ascending (ties keep index order), Z columns = eigenvectors.
 // Returns 0, or nonzero if n > KR_EIG_MAX or an eigenvalue needed more than 60
 // sweeps (the caller then falls back to Jacobi).
-KR_DEV int block_sym_eig_ql(int n, double *A, double *w, double *Z, int *ord) {
-  __shared__ double s_d[KR_EIG_MAX], s_e[KR_EIG_MAX], s_c[KR_EIG_MAX], s_s[KR_EIG_MAX];
+template <class G, int NMAX> KR_DEV int sym_eig_ql(int n, double *A, double *w, double *Z, int *ord) {
+  __shared__ double s_d[NMAX], s_e[NMAX], s_c[NMAX], s_s[NMAX];
   __shared__ double s_red[KR_MAX_WARPS];
   __shared__ int s_m, s_lo, s_fail;
   __shared__ double s_tn;
-  const int tid = threadIdx.x, bd = blockDim.x, lane = tid & 31, wid = tid >> 5, nw = bd >> 5;
-  if (n > KR_EIG_MAX || n < 1)
+  const int tid = G::tid(), bd = G::size(), lane = tid & 31, wid = tid >> 5, nw = bd >> 5;
+  if (n > NMAX || n < 1)
     return -1;
   // ---- 1) Householder reduction: column k below the subdiagonal -> alpha e1
   for (int k = 0; k + 2 < n; k++) {
@@ -266,7 +281,7 @@ KR_DEV int block_sym_eig_ql(int n, double *A, double *w, double *Z, int *ord) {
     double t2 = 0.0;
     for (int i = 1 + tid; i < r; i += bd)
       t2 += x[i] * x[i];
-    t2 = blk_allsum(t2, s_red);
+    t2 = G::allsum(t2, s_red);
     const double x0 = x[0];
     if (!(t2 > 0.0)) { // nothing to annihilate: H_k = I
       if (tid == 0) {
@@ -274,20 +289,20 @@ KR_DEV int block_sym_eig_ql(int n, double *A, double *w, double *Z, int *ord) {
         s_e[k] = x0;
         s_s[k] = 0.0;
       }
-      __syncthreads();
+      G::sync();
       continue;
     }
     const double sig = sqrt(x0 * x0 + t2);
     const double alpha = x0 >= 0.0 ? -sig : sig;
     const double beta = 1.0 / (sig * (sig + fabs(x0))); // H = I - beta v v^T, v = x - alpha e1
-    __syncthreads();
+    G::sync();
     if (tid == 0) {
       x[0] = x0 - alpha;
       s_d[k] = A[k + (size_t)k * n];
       s_e[k] = alpha;
       s_s[k] = beta;
     }
-    __syncthreads();
+    G::sync();
     // p = beta * A_sub v (A_sub symmetric: row i read as column i, coalesced)
     double *pv = s_c;
     for (int i = wid; i < r; i += nw) {
@@ -299,21 +314,21 @@ KR_DEV int block_sym_eig_ql(int n, double *A, double *w, double *Z, int *ord) {
       if (lane == 0)
         pv[i] = beta * acc;
     }
-    __syncthreads();
+    G::sync();
     double vp = 0.0;
     for (int i = tid; i < r; i += bd)
       vp += x[i] * pv[i];
-    vp = blk_allsum(vp, s_red);
+    vp = G::allsum(vp, s_red);
     const double K = 0.5 * beta * vp;
     for (int i = tid; i < r; i += bd)
       pv[i] -= K * x[i]; // w = p - K v
-    __syncthreads();
+    G::sync();
     // A_sub -= v w^T + w v^T
     for (int e = tid; e < r * r; e += bd) {
       const int j = e / r, i = e % r;
       A[r0 + i + (size_t)(r0 + j) * n] -= x[i] * pv[j] + pv[i] * x[j];
     }
-    __syncthreads();
+    G::sync();
   }
   if (tid == 0) {
     if (n >= 2) {
@@ -331,7 +346,7 @@ KR_DEV int block_sym_eig_ql(int n, double *A, double *w, double *Z, int *ord) {
   // ---- 2) Z = H_0 H_1 ... H_{n-3}, accumulated backwards
   for (int e = tid; e < n * n; e += bd)
     Z[e] = (e % n == e / n) ? 1.0 : 0.0;
-  __syncthreads();
+  G::sync();
   for (int k = n - 3; k >= 0; k--) {
     const double beta = s_s[k];
     if (beta == 0.0)
@@ -347,7 +362,7 @@ KR_DEV int block_sym_eig_ql(int n, double *A, double *w, double *Z, int *ord) {
       for (int i = lane; i < r; i += 32)
         zc[i] -= acc * v[i];
     }
-    __syncthreads();
+    G::sync();
   }
   // ---- 3) implicit QL on (d, e), rotations applied to the rows of Z
   for (int l = 0; l < n; l++) {
@@ -400,9 +415,9 @@ KR_DEV int block_sym_eig_ql(int n, double *A, double *w, double *Z, int *ord) {
           }
         }
       }
-      __syncthreads();
+      G::sync();
       const int m = s_m, lo = s_lo, fl = s_fail;
-      __syncthreads(); // all have read before thread 0 writes the next sweep
+      G::sync(); // all have read before thread 0 writes the next sweep
       if (m == l || fl)
         break;
       // rotation i mixes columns i and i+1 of every row, for i = m-1 down to
@@ -433,14 +448,14 @@ KR_DEV int block_sym_eig_ql(int n, double *A, double *w, double *Z, int *ord) {
         }
         Z[row + (size_t)lo * n] = xr;
       }
-      __syncthreads();
+      G::sync();
     }
     if (s_fail)
       break;
-    __syncthreads();
+    G::sync();
   }
   const int fail = s_fail;
-  __syncthreads();
+  G::sync();
   if (fail)
     return 1;
   // ---- 4) ascending order (ties by index), columns permuted through A
@@ -454,18 +469,36 @@ KR_DEV int block_sym_eig_ql(int n, double *A, double *w, double *Z, int *ord) {
     }
     ord[rank] = i;
   }
-  __syncthreads();
+  G::sync();
   for (int i = tid; i < n; i += bd)
     w[i] = s_d[ord[i]];
   for (int e = tid; e < n * n; e += bd) {
     const int j = e / n, row = e % n;
     A[row + (size_t)j * n] = Z[row + (size_t)ord[j] * n];
   }
-  __syncthreads();
+  G::sync();
   for (int e = tid; e < n * n; e += bd)
     Z[e] = A[e];
-  __syncthreads();
+  G::sync();
   return 0;
+}
+
+// The block's entry: warp 0 alone for n <= 32, else the whole block. Every
+// thread of the block calls it and gets the same return value.
+KR_DEV int block_sym_eig_ql(int n, double *A, double *w, double *Z, int *ord) {
+  if (n <= 32) {
+    __shared__ int s_rc;
+    if (threadIdx.x < 32) {
+      const int rc = sym_eig_ql<EigWarp, 32>(n, A, w, Z, ord);
+      if (threadIdx.x == 0)
+        s_rc = rc;
+    }
+    __syncthreads();
+    const int rc = s_rc;
+    __syncthreads();
+    return rc;
+  }
+  return sym_eig_ql<EigBlock, KR_EIG_MAX>(n, A, w, Z, ord);
 }
 
 // In-place Cholesky of the lower triangle of A (n x n, ld n). Returns 0 on

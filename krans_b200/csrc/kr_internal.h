@@ -119,6 +119,22 @@ void dev_free(krans_ctx *ctx, void *p, size_t bytes);
 // for the whole device. The served paths use them so that releasing one
 // finished launch never waits for a persistent launch still resident.
 int dev_alloc_async(krans_ctx *ctx, void **p, size_t bytes, cudaStream_t s);
+// Loads every kernel of the library into the context when it is created.
+// With CUDA's lazy module loading (the default), the first launch of a kernel
+// loads it, and loading may wait for the kernels already running: a first
+// launch beside a resident persistent launch (a new precision or solver in
+// the server, a standalone SpMV) would wait until that launch ends. Each
+// kernel translation unit lists its kernels in a preload_* function.
+void preload(const void *kernel);
+void preload_capi_kernels();
+void preload_spmv_kernels();
+void preload_gram_kernels();
+void preload_batch_cta_kernels();
+void preload_batch_cluster_kernels();
+void preload_cyclic_grid_kernels();
+void preload_lobpcg_kernels();
+void preload_lobpcg_cta_kernels();
+void preload_lobpcg_cluster_kernels();
 void dev_free_async(krans_ctx *ctx, void *p, size_t bytes, cudaStream_t s);
 int pick_lanes(int64_t rows, int64_t nnz);
 // threads per row of the solvers' SpMV from the context's tuning table

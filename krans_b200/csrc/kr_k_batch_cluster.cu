@@ -58,4 +58,9 @@ cudaError_t launch_cyclic_batch_cluster(bool mixed, int nclusters, int csize, si
                             stride_large, reqs_small, n_small, queue_small, ws_small, stride_small, feed, feed_large);
 }
 
+void preload_batch_cluster_kernels() {
+  preload(cl_kernel(true));
+  preload(cl_kernel(false));
+}
+
 } // namespace kr

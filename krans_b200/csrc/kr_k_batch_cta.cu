@@ -28,4 +28,9 @@ cudaError_t launch_cyclic_batch_cta(bool mixed, int grid, int block, size_t dyn_
   return cudaGetLastError();
 }
 
+void preload_batch_cta_kernels() {
+  preload((const void *)cyclic_batch_kernel<float>);
+  preload((const void *)cyclic_batch_kernel<double>);
+}
+
 } // namespace kr

@@ -25,4 +25,9 @@ cudaError_t launch_cyclic_grid(bool mixed, const CyclicDesc &d, int blocks, int 
   return cudaLaunchCooperativeKernel(grid_kernel(mixed), dim3(blocks), dim3(threads), args, 0, s);
 }
 
+void preload_cyclic_grid_kernels() {
+  preload((const void *)cyclic_grid_kernel<float>);
+  preload((const void *)cyclic_grid_kernel<double>);
+}
+
 } // namespace kr

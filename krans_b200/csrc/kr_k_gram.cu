@@ -65,6 +65,12 @@ static int coop_scratch(krans_ctx *ctx, int blocks, size_t part_doubles, char **
   return KRANS_OK;
 }
 
+void preload_gram_kernels() {
+  preload((const void *)block_gram_kernel);
+  preload((const void *)block_gemm_tn_kernel);
+  preload((const void *)block_combine_kernel);
+}
+
 } // namespace kr
 
 using namespace kr;

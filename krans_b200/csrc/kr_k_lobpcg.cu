@@ -41,4 +41,6 @@ cudaError_t launch_lobpcg(bool grid, const LobpcgDesc &d, const LobpcgDesc *d_de
   return launch_lobpcg_cta(d_dev, threads, s);
 }
 
+void preload_lobpcg_kernels() { preload((const void *)lobpcg_grid_kernel); }
+
 } // namespace kr

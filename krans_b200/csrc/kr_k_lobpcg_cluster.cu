@@ -49,4 +49,9 @@ cudaError_t launch_basis_max_residual(const CsrView &F, const double *basis, int
   return cudaGetLastError();
 }
 
+void preload_lobpcg_cluster_kernels() {
+  preload((const void *)lobpcg_cluster_kernel);
+  preload((const void *)basis_max_residual_kernel);
+}
+
 } // namespace kr

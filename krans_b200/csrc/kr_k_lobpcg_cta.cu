@@ -14,4 +14,6 @@ cudaError_t launch_lobpcg_cta(const LobpcgDesc *d_dev, int threads, cudaStream_t
   return cudaGetLastError();
 }
 
+void preload_lobpcg_cta_kernels() { preload((const void *)lobpcg_cta_kernel); }
+
 } // namespace kr

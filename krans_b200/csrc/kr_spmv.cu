@@ -312,4 +312,25 @@ cudaError_t spmv_launch(const SpmvOperand &A, bool fp32, const double *x, double
   return xl ? spmv_launch_t<double, true>(A, A.v64, x, y, sms, s) : spmv_launch_t<double, false>(A, A.v64, x, y, sms, s);
 }
 
+void preload_spmv_kernels() {
+  const void *ks[] = {
+      (const void *)spmv_uniform_kernel<1, double, false>, (const void *)spmv_uniform_kernel<2, double, false>,
+      (const void *)spmv_uniform_kernel<4, double, false>, (const void *)spmv_uniform_kernel<1, double, true>,
+      (const void *)spmv_uniform_kernel<2, double, true>,  (const void *)spmv_uniform_kernel<4, double, true>,
+      (const void *)spmv_uniform_kernel<1, float, false>,  (const void *)spmv_uniform_kernel<2, float, false>,
+      (const void *)spmv_uniform_kernel<4, float, false>,  (const void *)spmv_uniform_kernel<1, float, true>,
+      (const void *)spmv_uniform_kernel<2, float, true>,   (const void *)spmv_uniform_kernel<4, float, true>,
+      (const void *)spmv_rowtile_kernel<1, double, false>, (const void *)spmv_rowtile_kernel<2, double, false>,
+      (const void *)spmv_rowtile_kernel<4, double, false>, (const void *)spmv_rowtile_kernel<8, double, false>,
+      (const void *)spmv_rowtile_kernel<1, double, true>,  (const void *)spmv_rowtile_kernel<2, double, true>,
+      (const void *)spmv_rowtile_kernel<4, double, true>,  (const void *)spmv_rowtile_kernel<8, double, true>,
+      (const void *)spmv_rowtile_kernel<1, float, false>,  (const void *)spmv_rowtile_kernel<2, float, false>,
+      (const void *)spmv_rowtile_kernel<4, float, false>,  (const void *)spmv_rowtile_kernel<8, float, false>,
+      (const void *)spmv_rowtile_kernel<1, float, true>,   (const void *)spmv_rowtile_kernel<2, float, true>,
+      (const void *)spmv_rowtile_kernel<4, float, true>,   (const void *)spmv_rowtile_kernel<8, float, true>,
+      (const void *)spmv_lanes_kernel<double>,             (const void *)spmv_lanes_kernel<float>};
+  for (const void *k : ks)
+    preload(k);
+}
+
 } // namespace kr

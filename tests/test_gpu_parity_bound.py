@@ -153,10 +153,20 @@ def test_cyclic_planted_mixed_vs_fp64_oracle(ctx, oracle, k, ncv):
     O = oracle.cyclic(oracle.Csr.from_scipy(A), oracle.Rng(42), **opt)
     assert R.converged_to_target and O.converged_to_target
     assert R.fp64_fallback and 0 <= R.fallback_from < k
-    check_basis(oracle, A, U, O.right_null)
-    # the planted basis (columns of [W; -I_k], W sparse) has exact zeros, which make its pivoted RREF
-    # ill-posed (pivot choices flip under rounding): compared by subspace
-    # distance only (the RREF compare against the oracle's basis holds above)
+    # The planted null space (columns of [W; -I_k], W with 4 entries per
+    # column) is exactly zero in all but 4k of its first n-k coordinates. The
+    # RREF compare's pivot test is absolute (1e-12), so it is decided by the
+    # rounding noise a basis carries in those coordinates, and the vectors the
+    # mixed run accepted (accurate to ||Au|| <= 1e-12 L, not to 1e-14 per
+    # coordinate) carry more of it than the oracle's: measured, RREF
+    # differences above 1e-8 with principal-angle distances within 1e-10. This
+    # test therefore compares by the principal-angle distance, to the
+    # oracle's basis and to the analytic kernel, without the RREF compare.
+    L = norm_bound(A)
+    assert U.shape == O.right_null.shape
+    assert max(np.linalg.norm(A @ u) for u in U) / L <= RESID
+    assert oracle.max_pairwise_abs_dot(U) <= 1e-12
+    assert oracle.subspace_dist(O.right_null, U) <= DIST
     assert oracle.subspace_dist(inst.kernel, U) <= DIST
     # per vector: distance of each mixed-precision vector from the FP64 basis
     P = O.right_null
