@@ -315,7 +315,10 @@ KR_DEV void team_multidot(Team &tm, int64_t len, const TS *S, int64_t ld, int ns
   __syncthreads();
 }
 
-// w -= sum_q S_q * coef[q]  (coef in shared memory), optional ||w||^2 out.
+// w -= sum_q S_q * coef[q]  (coef in shared memory). The subtractions run in
+// q order for every element; the loads of several q are issued before their
+// subtractions, so a thread keeps 8-16 loads in flight instead of waiting out
+// one load per q (the short vectors of small solves are latency-bound on this).
 template <class Team, class TS, class TW>
 KR_DEV void team_multi_axpy(Team &tm, int64_t len, const TS *S, int64_t ld, int ns,
                             const double *coef, TW *w) {
@@ -326,7 +329,23 @@ KR_DEV void team_multi_axpy(Team &tm, int64_t len, const TS *S, int64_t ld, int 
 #pragma unroll
     for (int u = 0; u < 4; u++)
       acc[u] = to_d(w[i + u * nt]);
-    for (int q = 0; q < ns; q++) {
+    int q = 0;
+    for (; q + 3 < ns; q += 4) {
+      double sv[4][4];
+#pragma unroll
+      for (int t = 0; t < 4; t++)
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+          sv[t][u] = to_d(S[(int64_t)(q + t) * ld + i + u * nt]);
+#pragma unroll
+      for (int t = 0; t < 4; t++) {
+        const double cq = coef[q + t];
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+          acc[u] -= sv[t][u] * cq;
+      }
+    }
+    for (; q < ns; q++) {
       const double cq = coef[q];
       const TS *sq = S + (int64_t)q * ld + i;
       double sv[4];
@@ -343,7 +362,17 @@ KR_DEV void team_multi_axpy(Team &tm, int64_t len, const TS *S, int64_t ld, int 
   }
   for (; i < len; i += nt) {
     double acc = to_d(w[i]);
-    for (int q = 0; q < ns; q++)
+    int q = 0;
+    for (; q + 7 < ns; q += 8) {
+      double sv[8];
+#pragma unroll
+      for (int t = 0; t < 8; t++)
+        sv[t] = to_d(S[(int64_t)(q + t) * ld + i]);
+#pragma unroll
+      for (int t = 0; t < 8; t++)
+        acc -= sv[t] * coef[q + t];
+    }
+    for (; q < ns; q++)
       acc -= to_d(S[(int64_t)q * ld + i]) * coef[q];
     w[i] = (TW)acc;
   }

@@ -14,7 +14,8 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 def test_reference_arm_json_line():
     sys.path.insert(0, ROOT)
     import bench
-    # seed 3, batch 4: the one sampled instance is the smallest (nnz 2270)
+    # seed 3, batch 4, one step: one sampled instance per host core, drawn from
+    # the four instances of the batch
     out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "1",
                           "--warmup", "0", "--batch", "4", "--seed", "3"],
                          capture_output=True, text=True, timeout=900, cwd=ROOT)
@@ -24,7 +25,8 @@ def test_reference_arm_json_line():
     assert line["metric"] == bench.METRIC and line["unit"] == "solves/s" and line["higher_is_better"] is True
     assert line["value"] > 0 and line["cpu_baseline"]["value"] == line["value"]
     assert line["cpu_baseline"]["kind"] == ("reference" if bench._ref_available() else "port")
-    assert line["cpu_baseline"]["cores"] >= 1 and line["sampled"] == 1 and line["converged"] == 1
+    count = max(1, os.cpu_count() or 1)
+    assert line["cpu_baseline"]["cores"] >= 1 and line["sampled"] == count and line["converged"] == count
     assert line["e2e"] == {"value": line["value"], "unit": "solves/s", "h2d_bytes_per_step": 0,
                            "d2h_bytes_per_step": 0}
 
@@ -39,7 +41,10 @@ def test_reference_sample_and_rate():
     batches = bench.make_batches(3 + 5, 16, 9)
     s1, S = bench.reference_sample(batches, 3, 5, 9)
     s2, _ = bench.reference_sample(batches, 3, 5, 9)
-    assert s1 == s2 and S == 5 and [x[0] for x in s1] == [3, 4, 5, 6, 7]
+    count = max(5, os.cpu_count() or 1)  # at least one instance per host core
+    assert s1 == s2 and len(s1) == count and S == min(8, count)
+    assert [x[0] for x in s1] == [3 + q % 5 for q in range(count)]
+    assert [x[2] for x in s1] == [q % S for q in range(count)]
     for (st, i, j) in s1:  # the instance lies in its stratum of the step's batch
         order = sorted(range(16), key=lambda q: (batches[st][q].A.nnz, q))
         assert (j * 16) // S <= order.index(i) < ((j + 1) * 16) // S
