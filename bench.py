@@ -636,7 +636,8 @@ def run_lobpcg_incidence(args):
                      "unit": "GB/s", "frac": R.algo_bytes / T / 1e9 / peak, "traffic": None},
         "gram_tflops": R.gram_flops / T / 1e12,
         "phase_ms": {"apply_normal": R.phase_ms[0], "gram": R.phase_ms[1], "tiny_gep": R.phase_ms[2],
-                     "orthonormalise": R.phase_ms[3], "rest": R.phase_ms[4]},
+                     "orthonormalise": R.phase_ms[3], "rest": R.phase_ms[4],
+                     "rest_final_polish": R.final_polish_ms},
         "clocks": clocks, "gpu_launches": 1,
     }
     if not args.no_cpu_baseline:

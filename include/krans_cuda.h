@@ -335,6 +335,8 @@ typedef struct krans_lobpcg_result {
   double device_ms;
   double phase_ms[5]; /* device time (ms): apply_normal (SpMV pairs), Gram, tiny GEP,
                          orthonormalisation, the rest */
+  double final_polish_ms; /* part of the rest: the closing block_rr_polish, two_vec_rr_sharpen
+                             and MGS of the accepted basis (their operator products included) */
 } krans_lobpcg_result;
 
 int krans_cyclic_opts_init(krans_cyclic_opts *o);

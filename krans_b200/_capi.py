@@ -99,7 +99,8 @@ class LobpcgResultC(C.Structure):
                 ("best_unaccepted_residual", C.c_double), ("block_size", C.c_int64),
                 ("converged_to_target", C.c_int32), ("status", C.c_int32),
                 ("spmv", C.c_int64), ("spmvT", C.c_int64), ("algo_bytes", C.c_double),
-                ("gram_flops", C.c_double), ("device_ms", C.c_double), ("phase_ms", C.c_double * 5)]
+                ("gram_flops", C.c_double), ("device_ms", C.c_double), ("phase_ms", C.c_double * 5),
+                ("final_polish_ms", C.c_double)]
 
 
 class Request(C.Structure):

@@ -450,6 +450,7 @@ class LOBPCGResult:
     gram_flops: float = 0.0
     device_ms: float = 0.0
     phase_ms: tuple = ()
+    final_polish_ms: float = 0.0  # part of the last phase: closing polish, sharpening and MGS
 
 
 def _require(A, vf):
@@ -525,7 +526,7 @@ def find_nullspace_lobpcg_ex(A: CudaCsrMatrixAdapter, vf: CudaVectorFactory,
         best_unaccepted_residual=res.best_unaccepted_residual, block_size=res.block_size,
         converged_to_target=bool(res.converged_to_target), spmv=res.spmv, spmvT=res.spmvT,
         algo_bytes=res.algo_bytes, gram_flops=res.gram_flops, device_ms=res.device_ms,
-        phase_ms=tuple(res.phase_ms))
+        phase_ms=tuple(res.phase_ms), final_polish_ms=res.final_polish_ms)
 
 
 def find_nullspace_lobpcg(A, vf, opt) -> List[CudaVectorAdapter]:

@@ -792,6 +792,7 @@ template <class Team> struct LobpcgSolver {
     R.block_size = bs;
     double *X = d.X, *AX = d.AX, *Rb = d.Rb, *W = d.W, *P = d.P, *T1 = d.T1, *T2 = d.T2;
     int64_t nlocked = 0, nright = 0, its = 0;
+    uint64_t t_pol0 = 0; // start of the closing polish (0: not reached)
     const uint64_t t_run0 = globaltimer_ns();
 
     // ||A||_F estimate (LOBPCGSolver.cpp:163-178)
@@ -996,6 +997,7 @@ template <class Team> struct LobpcgSolver {
     }
     R.converged = (R.locked >= k_target) ? 1 : 0;
 
+    t_pol0 = globaltimer_ns();
     if (nright > 0 && tm.ok()) {
       const double desired = fmax(o.tol_abs, o.tol_rel * fmax(1.0, R.frob));
       const double target = fmax(1e-14, fmin(1e-10, 0.01 * desired));
@@ -1010,6 +1012,8 @@ template <class Team> struct LobpcgSolver {
     }
   finish:
     tm.sync();
+    if (t_pol0)
+      R.final_polish_ms = (double)(globaltimer_ns() - t_pol0) * 1e-6;
     if (tm.leader()) {
       R.n_right = nright;
       R.status = *(volatile int *)d.status;

@@ -271,6 +271,7 @@ extern "C" int krans_solve_lobpcg(krans_ctx *ctx, const krans_mat *A, krans_rng 
   result->device_ms = ms;
   for (int i = 0; i < 5; i++)
     result->phase_ms[i] = R.phase_ms[i];
+  result->final_polish_ms = R.final_polish_ms;
   if (R.err_code != kLobErrNone) {
     dev_free(ctx, ws, bytes);
     set_error("%s", lobpcg_err_msg(R.err_code));

@@ -214,6 +214,7 @@ struct LobpcgDevResult {
   int64_t spmv, spmvT;
   double bytes, gram_flops;
   double phase_ms[5]; // device time in: apply_normal, Gram, tiny GEP, orthonormalisation, the rest
+  double final_polish_ms; // part of the rest: the closing polish, sharpening and MGS
 };
 
 // error codes of the reference's throws (reported as KRANS_ERR_RUNTIME)
