@@ -988,12 +988,30 @@ def _stream(ctx, pool, mats, bounds, rate, seconds, precision, max_inflight, max
             srv.cancel(t)
         except KransError:
             pass  # finished meanwhile
+    # drain: every cancelled request must unwind; the scheduler's state goes
+    # to stderr every 10 s meanwhile, and a drain that takes over 300 s is
+    # reported instead of waited for
     t_c = time.perf_counter()
-    srv.drain(900.0)
-    print(f"serving: window closed at {elapsed:.1f}s, {unfinished} cancelled, drained in "
-          f"{time.perf_counter() - t_c:.1f}s", file=sys.stderr, flush=True)
-    srv.close()
+    drained, last = False, None
+    while time.perf_counter() - t_c < 300.0:
+        st = srv.stats()
+        last = st if st is not None else last
+        if st is not None and st[0] == 0 and st[1] == 0:
+            drained = True
+            break
+        if int(time.perf_counter() - t_c) % 10 == 0:
+            print(f"serving: draining {time.perf_counter() - t_c:.0f}s: queued/launches/lobpcg/running = {st}",
+                  file=sys.stderr, flush=True)
+        time.sleep(1.0)
+    print(f"serving: window closed at {elapsed:.1f}s, {unfinished} cancelled, "
+          f"{'drained' if drained else 'NOT drained'} in {time.perf_counter() - t_c:.1f}s (state {last})",
+          file=sys.stderr, flush=True)
+    if drained:
+        srv.drain(60.0)
+        srv.close()
     return {"offered": offered, "offered_rate": rate, "completed": done, "met_1e-12": ok, "window_s": elapsed,
+            "drained_after_cancel": drained, "drain_s": time.perf_counter() - t_c,
+            "scheduler_state_at_end": last,
             "sustained_solves_per_s": done / elapsed,
             "p50_ms": percentile(lat, 50), "p99_ms": percentile(lat, 99),
             "p50_ms_cyclic": percentile(lat_kind["cyclic"], 50), "p50_ms_lobpcg": percentile(lat_kind["lobpcg"], 50),
@@ -1017,6 +1035,14 @@ def run_serving(args):
     bounds = [1e-12 * lower_norm_bound(inst.A) for inst, _ in pool]
     budget = 150 * 10**9
     high, clk_high = _clocked(lambda: _stream(ctx, pool, mats, bounds, args.rate, args.seconds, 1, 4, 1024, 11, budget))
+    if not high["drained_after_cancel"]:
+        # requests still on the device: report what was measured and stop here
+        # (the server cannot be destroyed under them, nor the next phase run)
+        print(json.dumps({"metric": "serving stream: sustained null-space solves/s and p50/p99 latency incl. "
+                                    "queueing", "value": high["sustained_solves_per_s"], "unit": "solves/s",
+                          "higher_is_better": True, "n_gpus": 1, "oversubscribed": high,
+                          "error": "the drain after cancelling did not finish within 300 s"}), flush=True)
+        os._exit(0)
     low_rate = max(0.05, 0.5 * high["sustained_solves_per_s"])
     low, clk_low = _clocked(lambda: _stream(ctx, pool, mats, bounds, low_rate, args.seconds, 1, 4, 1024, 12, budget))
     base = _stream(ctx, pool, mats, bounds, low_rate, args.seconds, 0, 1, 1, 12, budget)

@@ -467,6 +467,12 @@ int krans_cancel(krans_server *s, uint64_t ticket);
 int krans_server_completed(krans_server *s, uint64_t *tickets, int64_t capacity, int64_t *count);
 /* Block until every submitted request has finished or timeout_ms passes. */
 int krans_server_drain(krans_server *s, double timeout_ms);
+/* Scheduler state: out[0] queued tickets (cancelled ones not yet dropped
+ * included), out[1] launches in flight, out[2] of them LOBPCG, out[3] cyclic
+ * requests published into running launches and not finished. Returns
+ * KRANS_ERR_TIMEOUT at once, without waiting, while the scheduler holds its
+ * lock. */
+int krans_server_stats(krans_server *s, int64_t out[4]);
 
 #ifdef __cplusplus
 }

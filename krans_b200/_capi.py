@@ -191,6 +191,7 @@ SIGNATURES = {
     "krans_poll": [P, C.c_uint64, C.POINTER(I), C.POINTER(RequestResult)],
     "krans_cancel": [P, C.c_uint64],
     "krans_server_drain": [P, D],
+    "krans_server_stats": [P, C.POINTER(I64)],
     "krans_server_completed": [P, C.POINTER(C.c_uint64), I64, C.POINTER(I64)],
 }
 _RESTYPE = {"krans_last_error": C.c_char_p, "krans_version": C.c_char_p, "krans_host_free": None}

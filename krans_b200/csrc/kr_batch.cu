@@ -1228,6 +1228,26 @@ int krans_server_completed(krans_server *s, uint64_t *tickets, int64_t capacity,
   return KRANS_OK;
 }
 
+int krans_server_stats(krans_server *s, int64_t out[4]) {
+  KR_CHECK_ARG(s && out, "krans_server_stats: NULL argument");
+  std::unique_lock<std::mutex> lk(s->mu, std::try_to_lock);
+  if (!lk.owns_lock()) {
+    set_error("krans_server_stats: the scheduler holds its lock");
+    return KRANS_ERR_TIMEOUT;
+  }
+  out[0] = (int64_t)s->queue.size();
+  out[1] = (int64_t)s->inflight.size();
+  out[2] = 0;
+  out[3] = 0;
+  for (const InFlight *f : s->inflight) {
+    if (f->lob)
+      out[2]++;
+    else
+      out[3] += (int64_t)f->running.size();
+  }
+  return KRANS_OK;
+}
+
 int krans_server_drain(krans_server *s, double timeout_ms) {
   KR_CHECK_ARG(s, "krans_server_drain: NULL argument");
   std::unique_lock<std::mutex> lk(s->mu);

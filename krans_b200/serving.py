@@ -133,6 +133,13 @@ class Server:
         check(self.ctx.lib.krans_server_completed(self.h, buf, capacity, C.byref(n)), "krans_server_completed")
         return [int(buf[i]) for i in range(n.value)]
 
+    def stats(self):
+        """(queued, launches in flight, LOBPCG launches, running cyclic
+        requests), or None while the scheduler holds its lock."""
+        out = (C.c_int64 * 4)()
+        rc = self.ctx.lib.krans_server_stats(self.h, out)
+        return tuple(int(x) for x in out) if rc == 0 else None
+
     def drain(self, timeout_s: float = 600.0):
         check(self.ctx.lib.krans_server_drain(self.h, timeout_s * 1e3), "krans_server_drain")
         for t in list(self.live):
