@@ -734,7 +734,6 @@ struct krans_server {
   }
   bool admit_lobpcg(uint64_t id, Clock::time_point now);
   bool admit_cyclic(Clock::time_point now);
-  bool feed_open(Clock::time_point now);
 };
 
 // LOBPCG request at the head of the queue: its own launch on a free stream.
@@ -809,8 +808,6 @@ bool krans_server::admit_cyclic(Clock::time_point now) {
       fail(id, r, now);
       return true;
     }
-    if (free_stream() < 0)
-      return false; // no stream for a launch of its own yet: the open launch stays open (feed_open)
     open->L.close(); // it does not fit: let the open launch drain, start the next one
     open = nullptr;
   }
@@ -910,55 +907,6 @@ bool krans_server::admit_cyclic(Clock::time_point now) {
   return true;
 }
 
-// The queue's head waits for a stream (its own launch: a LOBPCG request, or
-// a cyclic one of another precision or size than the open launch takes).
-// Meanwhile the open launch is fed the queued cyclic requests behind the head
-// that fit it, in queue order, from the first kFeedScan entries; the head
-// keeps its place. Without this, a request that needs a stream of its own
-// held up every request behind it while teams of the open launch sat idle.
-static const int kFeedScan = 1024;
-bool krans_server::feed_open(Clock::time_point now) {
-  if (!open || open->L.done() || queue.size() < 2)
-    return false;
-  // the requests' matrices finish their device set-up on the context's stream
-  cudaError_t ew = cudaEventRecord(ctx_ready, ctx->stream);
-  if (ew == cudaSuccess)
-    ew = cudaEventSynchronize(ctx_ready);
-  if (ew != cudaSuccess)
-    return false;
-  bool moved = false;
-  int scanned = 0, misses = 0;
-  for (auto it = std::next(queue.begin()); it != queue.end() && scanned < kFeedScan && misses < 64;) {
-    ++scanned;
-    ServerTicket &t = tickets[*it];
-    if (t.state == 4) { // cancelled while queued
-      it = queue.erase(it);
-      continue;
-    }
-    if (t.req.solver != KRANS_SOLVER_CYCLIC || t.req.opts.precision != open->L.precision) {
-      ++it;
-      continue;
-    }
-    int slot = -1;
-    const int r = open->L.try_publish(t.req, &slot);
-    if (r == 1) {
-      t.state = 1;
-      t.start_t = now;
-      open->running.push_back({*it, slot, now});
-      it = queue.erase(it);
-      moved = true;
-    } else if (r < 0) {
-      fail(*it, r, now);
-      it = queue.erase(it);
-      moved = true;
-    } else {
-      ++it; // its class of the open launch is full, or its workspace exceeds the class slot
-      ++misses;
-    }
-  }
-  return moved;
-}
-
 void krans_server::run() {
   cudaSetDevice(ctx->device);
   std::unique_lock<std::mutex> lk(mu);
@@ -1034,10 +982,8 @@ void krans_server::run() {
         continue;
       }
       const bool ok = t.req.solver == KRANS_SOLVER_LOBPCG ? admit_lobpcg(id, now) : admit_cyclic(now);
-      if (!ok) {
-        moved |= feed_open(now);
+      if (!ok)
         break;
-      }
       moved = true;
     }
     if (moved)
