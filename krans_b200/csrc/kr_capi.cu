@@ -30,18 +30,25 @@ int cuda_fail(cudaError_t e, const char *what, const char *file, int line) {
   return KRANS_ERR_CUDA;
 }
 
+static void release_bytes(krans_ctx *ctx, size_t bytes) {
+  size_t cur = ctx->in_use.load();
+  while (!ctx->in_use.compare_exchange_weak(cur, cur - std::min(cur, bytes))) {
+  }
+}
+
 int dev_alloc(krans_ctx *ctx, void **p, size_t bytes) {
   *p = nullptr;
   if (bytes == 0)
     bytes = 256;
-  if (ctx->budget && ctx->in_use + bytes > ctx->budget) {
-    set_error("HBM budget exceeded: %zu + %zu > %zu bytes", ctx->in_use, bytes, ctx->budget);
+  const size_t cur = ctx->in_use.load();
+  if (ctx->budget && cur + bytes > ctx->budget) {
+    set_error("HBM budget exceeded: %zu + %zu > %zu bytes", cur, bytes, ctx->budget);
     return KRANS_ERR_OUT_OF_MEMORY;
   }
   cudaError_t e = cudaMalloc(p, bytes);
   if (e != cudaSuccess)
     return cuda_fail(e, "cudaMalloc", __FILE__, __LINE__);
-  ctx->in_use += bytes;
+  ctx->in_use.fetch_add(bytes);
   return KRANS_OK;
 }
 
@@ -51,21 +58,22 @@ void dev_free(krans_ctx *ctx, void *p, size_t bytes) {
   if (bytes == 0)
     bytes = 256;
   cudaFree(p);
-  ctx->in_use -= std::min(ctx->in_use, bytes);
+  release_bytes(ctx, bytes);
 }
 
 int dev_alloc_async(krans_ctx *ctx, void **p, size_t bytes, cudaStream_t s) {
   *p = nullptr;
   if (bytes == 0)
     bytes = 256;
-  if (ctx->budget && ctx->in_use + bytes > ctx->budget) {
-    set_error("HBM budget exceeded: %zu + %zu > %zu bytes", ctx->in_use, bytes, ctx->budget);
+  const size_t cur = ctx->in_use.load();
+  if (ctx->budget && cur + bytes > ctx->budget) {
+    set_error("HBM budget exceeded: %zu + %zu > %zu bytes", cur, bytes, ctx->budget);
     return KRANS_ERR_OUT_OF_MEMORY;
   }
   cudaError_t e = cudaMallocAsync(p, bytes, s);
   if (e != cudaSuccess)
     return cuda_fail(e, "cudaMallocAsync", __FILE__, __LINE__);
-  ctx->in_use += bytes;
+  ctx->in_use.fetch_add(bytes);
   return KRANS_OK;
 }
 
@@ -75,7 +83,7 @@ void dev_free_async(krans_ctx *ctx, void *p, size_t bytes, cudaStream_t s) {
   if (bytes == 0)
     bytes = 256;
   cudaFreeAsync(p, s);
-  ctx->in_use -= std::min(ctx->in_use, bytes);
+  release_bytes(ctx, bytes);
 }
 
 // Threads per row of the SpMV. Short rows go one per thread: the gathers of
@@ -361,7 +369,7 @@ int krans_ctx_synchronize(krans_ctx *ctx) {
 
 int krans_ctx_memory_in_use(const krans_ctx *ctx, size_t *bytes) {
   KR_CHECK_ARG(ctx && bytes, "NULL argument");
-  *bytes = ctx->in_use;
+  *bytes = ctx->in_use.load();
   return KRANS_OK;
 }
 

@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdarg>
 #include <cstdint>
 #include <cstdio>
@@ -56,7 +57,7 @@ struct krans_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
   size_t budget = 0;
-  size_t in_use = 0;
+  std::atomic<size_t> in_use{0}; // device bytes allocated through dev_alloc* (the server thread allocates too)
   int sms = 0;
   int cc_major = 0, cc_minor = 0;
   double *h_scalar = nullptr; // pinned scalars for D2H reads
