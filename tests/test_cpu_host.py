@@ -48,6 +48,9 @@ def test_option_defaults_mirror_reference():
     assert (o.grad_max_iters, o.frob_samples, o.prescreen_factor, o.stagnation_restarts) == (3000, 4, 0.8, 30)
     c = o.to_c()
     assert c.ncv == 48 and c.reorth == 2 and c.stagnation_restarts == 30 and c.precision == 0
+    # engine knob: a mixed solve that stalls in its polish continues in FP64 unless told otherwise
+    assert o.mixed_fallback and c.mixed_fallback == 1
+    assert kb.CyclicLanczosOptions(mixed_fallback=False).to_c().mixed_fallback == 0
     L = kb.LOBPCGOptions()
     assert (L.nev, L.block_size, L.max_iters, L.restart, L.gs_tol) == (1, 0, 1000, 0.9, 1e-14)
     assert L.soft_locking and L.gs_reorth and L.frob_samples == 4 and L.nullity_known == -1
