@@ -50,6 +50,12 @@ typedef struct krans_rng krans_rng;
 const char *krans_last_error(void);
 /* Library version string. */
 const char *krans_version(void);
+/* sizeof of the ABI structs as this library was compiled, for bindings to
+ * check their layouts against: out[0..8] = krans_cyclic_opts,
+ * krans_cyclic_result, krans_lobpcg_opts, krans_lobpcg_result, krans_request,
+ * krans_request_result, krans_server_opts, krans_spmv_tuning,
+ * krans_batch_tuning. Returns the number of entries (9). */
+int krans_abi_sizes(int64_t *out, int capacity);
 
 /* ---- context --------------------------------------------------------------- */
 /* Opens `device`, creates the context's stream. hbm_budget_bytes = 0 means

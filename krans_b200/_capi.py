@@ -134,6 +134,7 @@ D = C.c_double
 SIGNATURES = {
     "krans_last_error": [],
     "krans_version": [],
+    "krans_abi_sizes": [C.POINTER(I64), C.c_int],
     "krans_ctx_create": [I, C.c_size_t, PP],
     "krans_ctx_destroy": [P],
     "krans_ctx_synchronize": [P],

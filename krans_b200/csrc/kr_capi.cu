@@ -292,6 +292,17 @@ extern "C" {
 const char *krans_last_error(void) { return kr::g_last_error.c_str(); }
 const char *krans_version(void) { return "krans_b200 0.1 (sm_100a)"; }
 
+int krans_abi_sizes(int64_t *out, int capacity) {
+  const int64_t sz[9] = {(int64_t)sizeof(krans_cyclic_opts),    (int64_t)sizeof(krans_cyclic_result),
+                         (int64_t)sizeof(krans_lobpcg_opts),    (int64_t)sizeof(krans_lobpcg_result),
+                         (int64_t)sizeof(krans_request),        (int64_t)sizeof(krans_request_result),
+                         (int64_t)sizeof(krans_server_opts),    (int64_t)sizeof(krans_spmv_tuning),
+                         (int64_t)sizeof(krans_batch_tuning)};
+  for (int i = 0; i < 9 && i < capacity && out; i++)
+    out[i] = sz[i];
+  return 9;
+}
+
 int krans_ctx_create(int device, size_t hbm_budget_bytes, krans_ctx **out) {
   KR_CHECK_ARG(out, "krans_ctx_create: out is NULL");
   *out = nullptr;

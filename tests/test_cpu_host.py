@@ -93,3 +93,16 @@ def _replica_worker(rank, world, out):
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     open(os.path.join(out, f"r{rank}"), "w").write(str(float(t)))
     dist.destroy_process_group()
+
+
+def test_abi_struct_sizes_match_the_library():
+    # the ctypes mirrors of the C ABI structs (krans_b200/_capi.py) against
+    # sizeof() as the library was compiled (krans_abi_sizes; no GPU needed)
+    import ctypes as C
+    from krans_b200 import _capi as K
+    lib = K.load()
+    out = (C.c_int64 * 9)()
+    assert lib.krans_abi_sizes(out, 9) == 9
+    mine = [K.CyclicOpts, K.CyclicResultC, K.LobpcgOpts, K.LobpcgResultC, K.Request, K.RequestResult,
+            K.ServerOpts, K.SpmvTuning, K.BatchTuning]
+    assert [C.sizeof(t) for t in mine] == list(out)
