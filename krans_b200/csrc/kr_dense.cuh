@@ -7,7 +7,10 @@
 //    one warp per column pair;
 //  - two-sided cyclic Jacobi for symmetric matrices, Brent-Luk parallel
 //    ordering (all disjoint rotations of a round applied at once);
-//  - right-looking Cholesky and a triangular inverse.
+//  - Householder tridiagonalisation + implicit QL for symmetric matrices;
+//  - Cholesky and a triangular inverse.
+// Orders up to 32 run on warp 0 with warp barriers (block barriers dominate
+// such tiny problems); larger ones use the whole block.
 // Matrices are column-major in global memory owned by the solve.
 #pragma once
 
