@@ -884,7 +884,8 @@ def serving_pool(P, nnz_lo, nnz_hi, kmax=64, seed=7):
       graph incidence, mean degree 8, k components (k uniform in 1..kmax),
           solved by block LOBPCG (the large-LOBPCG workload's generator)
       planted kernel A = [B | B W], 8 entries per row of B, k planted
-          (1..kmax), cyclic Lanczos in mixed precision (the planted workload's)
+          (1..kmax), cyclic Lanczos in FP64 (serving_opts: the mixed form
+          stalls on these)
       the batched workload's: a shift operator with N = k (1..16) or an
           incidence matrix of mean degree 6 with k components (1..16), cyclic,
           mixed precision.

@@ -67,3 +67,20 @@ def test_indicator_kernel_distance():
     V[0] += 1e-3 * np.random.default_rng(1).standard_normal(6)
     V = np.linalg.qr(V.T)[0].T
     assert 1e-5 < bench.kernel_dist_indicator(V, labels, 3) < 1e-2
+
+
+def test_serving_request_options():
+    # the serving stream's per-generator options: planted-kernel requests in
+    # FP64, the batched workload's in mixed precision, LOBPCG for incidence
+    sys.path.insert(0, ROOT)
+    import bench
+    import krans_b200 as kb
+    pool = bench.serving_pool(6, 1e4, 3e4, kmax=4)
+    kinds = {}
+    for inst, solver in pool:
+        o = bench.serving_opts(kb, inst, solver, 1)
+        kinds.setdefault((inst.name, solver), set()).add(
+            type(o).__name__ if solver == "lobpcg" else int(o.precision))
+    assert kinds[("planted", "cyclic")] == {0}
+    assert all(v == {1} for (name, solver), v in kinds.items() if solver == "cyclic" and name != "planted")
+    assert kinds[("incidence", "lobpcg")] == {"LOBPCGOptions"}
